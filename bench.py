@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the DVB-S2 LDPC decoder on B200 (and of the reference's CPU
+decoder on the same host).
+
+Workload (the configuration the headline metric is quoted on): DVB-S2 normal
+FECFRAMEs (n = 64800), code rate 3/5, 8PSK over AWGN with Es/N0 swept
+5.0 - 6.5 dB in 0.25 dB steps, int8 LLRs, layered min-sum with at most 30
+iterations and syndrome early stop, 4096 frames per launch.  One step = one
+decode launch over one 4096-frame batch of one Es/N0 point; the steps cycle
+through the seven points.  Inputs are seeded synthetic frames (the project's
+encoder, interleaver, 8PSK mapper, AWGN and max-log demapper), generated on
+the GPU before timing; each batch is 265 MB, above the 126 MB L2, so no L2
+flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  Under torchrun every rank decodes its own
+frames (weak scaling, no data-path collective); the time is the max over
+ranks of the CUDA-event time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LDPC info Gbit/s at matched FER: learned vs plain min-sum, 1xB200 vs host CPU"
+UNIT = "Gbit/s"
+RATE, SHORT, CONST = "3_5", 0, "8PSK"
+ESN0 = [5.0, 5.25, 5.5, 5.75, 6.0, 6.25, 6.5]
+MAX_ITER = 30
+SMEM_BYTES_PER_CLK = 128  # per SM
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=14)
+    ap.add_argument("--warmup", type=int, default=7)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--frames", type=int, default=4096, help="frames per step (launch)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--e2e-steps", type=int, default=7)
+    return ap.parse_args()
+
+
+def workload_config(frames, world):
+    return {
+        "workload": "dvbs2-normal-3_5-8psk-awgn-sweep",
+        "code": "DVB-S2 normal FECFRAME n=64800 rate 3/5 (kldpc=38880 info bits)",
+        "modulation": CONST,
+        "esn0_db": ESN0,
+        "frames_per_step": frames,
+        "max_iter": MAX_ITER,
+        "stopping": "per frame (syndrome before every iteration)",
+        "llr": "int8, 2 x max-log LLR saturated to +-127",
+        "l2": "inputs larger than L2 (265 MB per step), no flush",
+        "parallelism": "frames across persistent CTAs; %d rank(s), independent frame shards" % world,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def profiled_traffic():
+    """DRAM bytes per decode launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ldpc_decode_normal_3_5.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference decoder compiled from its sources (oracle/_ref)
+# ---------------------------------------------------------------------------
+
+def cpu_reference_run(llr_batches, seconds, threads):
+    """Reference production mode (rxmt.c:514-536): one thread per core, each
+    with its own handle, decoding batches of `lanes` frames with
+    drx_ldpc_decode.  Runs for about `seconds`; returns (frames/s, lanes,
+    frames, threads)."""
+    import oracle
+    lib = oracle.load_ref()
+    if lib is None:
+        raise RuntimeError("reference decoder not built (make -C oracle ref)")
+    lanes = lib.ref_ldpc_lanes()
+    counts = [0] * threads
+    stop_at = [0.0]
+    barrier = threading.Barrier(threads + 1)
+
+    def worker(w):
+        ref = oracle.RefCode(SHORT, RATE)
+        nb = len(llr_batches)
+        k = w
+        barrier.wait()
+        while time.perf_counter() < stop_at[0]:
+            batch = llr_batches[k % nb]
+            g0 = (k // nb * lanes) % max(1, batch.shape[0] - lanes + 1)
+            ref.decode_call(batch[g0:g0 + lanes], MAX_ITER)
+            counts[w] += lanes
+            k += threads
+
+    ts = [threading.Thread(target=worker, args=(w,)) for w in range(threads)]
+    for t in ts:
+        t.start()
+    t0 = time.perf_counter()
+    stop_at[0] = t0 + seconds
+    barrier.wait()
+    t0 = time.perf_counter()
+    for t in ts:
+        t.join()
+    dt = time.perf_counter() - t0
+    return sum(counts) / dt, lanes, sum(counts), threads
+
+
+def host_llr_batches(frames_per_point, seed=99):
+    """Input frames for the CPU-only arm, made on the CPU (numpy channel)."""
+    from oracle import OrcCode, datagen
+    code = OrcCode(SHORT, RATE)
+    out = []
+    for k, es in enumerate(ESN0):
+        d = datagen.make_frames(SHORT, RATE, frames_per_point, es, CONST, seed=seed + k, code=code)
+        out.append(d["llr"])
+    return out
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    import oracle
+    lib = oracle.load_ref()
+    if lib is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference decoder not built (oracle/_ref missing)"}))
+        return
+    lanes = lib.ref_ldpc_lanes()
+    batches = host_llr_batches(lanes)
+    # one step: every thread decodes one batch of `lanes` frames
+    import oracle as _o
+    refs = [_o.RefCode(SHORT, RATE) for _ in range(threads)]
+
+    def step(k):
+        def w(i):
+            refs[i].decode_call(batches[(k + i) % len(batches)], MAX_ITER)
+        ts = [threading.Thread(target=w, args=(i,)) for i in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+
+    for k in range(args.warmup):
+        step(k)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        step(args.warmup + k)
+    dt = time.perf_counter() - t0
+    frames = args.steps * threads * lanes
+    gbps = frames * 38880 / dt / 1e9
+    line = {
+        "metric": METRIC, "value": gbps, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+        "impl": "reference",
+        "config": dict(workload_config(lanes * threads, 1),
+                       stopping="per batch of %d frames (reference drx_ldpc_decode semantics)" % lanes,
+                       frames_per_step=lanes * threads),
+        "cpu_baseline": {"value": gbps, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "lanes": lanes,
+                         "sample": "%d steps x %d threads x one %d-frame drx_ldpc_decode call" % (
+                             args.steps, threads, lanes)},
+        "e2e": {"value": gbps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    import dvbrx_b200 as D
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    p = D.fec_lookup(SHORT, RATE)
+    dec = D.Ldpc(p, RATE)
+    F = args.frames
+    kldpc = p.kldpc
+    stream = torch.cuda.current_stream()
+
+    # inputs: one batch per Es/N0 point, resident in HBM
+    llr, info = [], []
+    for k, es in enumerate(ESN0):
+        l, inf, _ = dec.generate(F, es, seed=1000003 * (rank + 1) + k, constellation=CONST, info=True)
+        llr.append(l)
+        info.append(inf)
+    out = torch.empty((F, dec.nbytes), dtype=torch.uint8, device="cuda")
+    iters = [torch.empty(F, dtype=torch.int32, device="cuda") for _ in range(args.steps)]
+    oks = [torch.empty(F, dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
+    errs = torch.zeros(args.steps, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+
+    def step(k, it_buf, ok_buf):
+        dec.decode_device(llr[k % len(ESN0)], MAX_ITER, out=out, iters=it_buf, ok=ok_buf)
+
+    for k in range(args.warmup):
+        step(k, iters[0], oks[0])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        step(args.warmup + k, iters[k], oks[k])
+        ev[k][1].record(stream)
+        # frame errors of this step (outside the kernel's events)
+        errs[k] = (out != info[(args.warmup + k) % len(ESN0)]).any(dim=1).sum()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launch_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = ev[0][0].elapsed_time(ev[-1][1])
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+
+    it_all = torch.stack(iters).to(torch.int64)
+    iters_sum = int(it_all.sum().item())
+    frames_rank = args.steps * F
+    fer = float(errs.sum().item()) / frames_rank
+    value = world * frames_rank * kldpc / (total_ms * 1e-3) / 1e9
+
+    # roofline of the decode kernel (one launch per step)
+    edges = dec.info.edges
+    kern_s = statistics.mean(launch_ms) * 1e-3
+    smem_bytes = iters_sum / args.steps * 4 * edges
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    smem_peak = nsm * SMEM_BYTES_PER_CLK * 1965e6 / 1e9
+    hbm_bytes = F * (dec.N + dec.nbytes + 5)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    traffic = profiled_traffic()
+    roofline = {
+        "bound": "smem",
+        "kernel": "k_decode (drxg::k_decode<16,3>)",
+        "achieved": smem_bytes / kern_s / 1e9,
+        "peak": smem_peak,
+        "unit": "GB/s",
+        "frac": smem_bytes / kern_s / 1e9 / smem_peak,
+        "peak_source": "nominal: %d SMs x 128 B/clk x 1965 MHz (no shared-memory peak in MEASURED_PEAKS.json)" % nsm,
+        "algorithmic_bytes_per_launch": smem_bytes,
+        "bytes_per_unit": "4 x E = %d B per frame-iteration (E = %d edges)" % (4 * edges, edges),
+        "traffic": traffic,
+        "hbm": {"achieved": hbm_bytes / kern_s / 1e9, "peak": hbm_peak,
+                "frac": hbm_bytes / kern_s / 1e9 / hbm_peak, "unit": "GB/s",
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
+                "algorithmic_bytes_per_launch": hbm_bytes},
+        "avg_launch_ms": statistics.mean(launch_ms),
+        "sm_mhz_median": sm_mhz,
+    }
+
+    # end to end through the C ABI with host buffers (synchronous call)
+    e2e = None
+    if rank == 0 or world > 1:
+        host = [l.cpu().numpy() for l in llr]
+        for k in range(min(2, args.e2e_steps)):
+            dec.decode_host(host[k % len(host)], MAX_ITER)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for k in range(args.e2e_steps):
+            dec.decode_host(host[k % len(host)], MAX_ITER)
+        dt = time.perf_counter() - t0
+        tt = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dt = float(tt.item())
+        e2e = {"value": world * args.e2e_steps * F * kldpc / dt / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": F * dec.N,
+               "d2h_bytes_per_step": F * (dec.nbytes + 4 + 1),
+               "api": "drx_ldpc_decode_host (host rows in, host bits/iterations/flags out; wall clock)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            host_b = [l[: 4 * 64].cpu().numpy() for l in llr]
+            threads = os.cpu_count() or 1
+            fps, lanes, nf, thr = cpu_reference_run(host_b, args.cpu_seconds, threads)
+            fps1, _, _, _ = cpu_reference_run(host_b, min(3.0, args.cpu_seconds), 1)
+            cpu = {"value": fps * kldpc / 1e9, "unit": UNIT, "cores": thr, "kind": "reference",
+                   "lanes": lanes, "value_1core": fps1 * kldpc / 1e9,
+                   "sample": "%d frames in %.0f s: batches of %d frames (drx_ldpc_decode), one "
+                             "thread and handle per core, the same int8 LLRs as the GPU, all 7 Es/N0 points"
+                             % (nf, args.cpu_seconds, lanes)}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "failed: %s" % e}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+            "config": workload_config(F, world),
+            "decoder": "plain layered offset min-sum (bit-exact to the reference)",
+            "quality": {"fer": fer, "avg_iterations": iters_sum / frames_rank},
+            "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,221 @@
+"""dvbrx_b200 — DVB-S2/S2X/T2 LDPC decoding on one NVIDIA B200 (sm_100a).
+
+Python host side of ``libdvbrx_b200.so``.  The library's C ABI
+(``include/dvbrx_b200.h``) is the product: a drop-in for the reference
+receiver's ``drx_fec_lookup`` / ``drx_ldpc_new`` / ``drx_ldpc_decode`` /
+``drx_ldpc_free`` (TrusterBSW/DVB-Rx ``libdvbrx/include/dvbrx/ldpc.h:14-36``,
+``fec.h:13-25``) plus batch entry points.  This module binds it with ctypes,
+keeping the reference's names and argument meaning:
+
+    p = fec_lookup(False, "3_5")          # drx_fec_lookup
+    d = Ldpc(p, "3_5")                    # drx_ldpc_new
+    it = d.decode(llr_rows, out_rows, 30) # drx_ldpc_decode: iterations or -1
+
+There is no CPU fallback: without the built library, or without a CUDA
+device, every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdvbrx_b200.so")
+
+STOP_FRAME = 0  # DRX_STOP_FRAME
+
+_lib = None
+
+
+class FecParams(ctypes.Structure):
+    """``drx_fec_params`` (reference ``libdvbrx/include/dvbrx/fec.h:13-19``)."""
+
+    _fields_ = [
+        ("short_frame", ctypes.c_int),
+        ("nldpc", ctypes.c_int),
+        ("kldpc", ctypes.c_int),
+        ("kbch", ctypes.c_int),
+        ("t", ctypes.c_int),
+    ]
+
+    def __repr__(self):
+        return "FecParams(short_frame=%d, nldpc=%d, kldpc=%d, kbch=%d, t=%d)" % (
+            self.short_frame, self.nldpc, self.kldpc, self.kbch, self.t)
+
+
+class LdpcInfo(ctypes.Structure):
+    """``drx_ldpc_info``."""
+
+    _fields_ = [(n, ctypes.c_int) for n in
+                ("nldpc", "kldpc", "K", "R", "q", "edges", "steps", "deg_max", "levelled")]
+
+
+EXPORTS = (
+    "drx_fec_lookup", "drx_ldpc_lanes", "drx_ldpc_new", "drx_ldpc_free", "drx_ldpc_decode",
+    "drx_ldpc_last_error", "drx_ldpc_get_info", "drx_ldpc_decode_device", "drx_ldpc_decode_host",
+    "drx_ldpc_device_error", "drx_ldpc_code_info", "drx_channel_generate",
+)
+
+
+def lib():
+    """The loaded C-ABI library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("%s is missing: build it with `python -m dvbrx_b200.build`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, cp, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t
+        L.drx_fec_lookup.argtypes = [ip, cp, ctypes.POINTER(FecParams)]
+        L.drx_fec_lookup.restype = ip
+        L.drx_ldpc_lanes.restype = ip
+        L.drx_ldpc_new.argtypes = [ctypes.POINTER(FecParams), cp]
+        L.drx_ldpc_new.restype = vp
+        L.drx_ldpc_free.argtypes = [vp]
+        L.drx_ldpc_decode.argtypes = [vp, vp, vp, ip, ip]
+        L.drx_ldpc_decode.restype = ip
+        L.drx_ldpc_last_error.restype = cp
+        L.drx_ldpc_get_info.argtypes = [vp, ctypes.POINTER(LdpcInfo)]
+        L.drx_ldpc_get_info.restype = ip
+        L.drx_ldpc_decode_device.argtypes = [vp, vp, sz, vp, sz, vp, vp, ip, ip, ip, vp]
+        L.drx_ldpc_decode_device.restype = ip
+        L.drx_ldpc_decode_host.argtypes = [vp, vp, vp, vp, vp, ip, ip, ip]
+        L.drx_ldpc_decode_host.restype = ip
+        L.drx_ldpc_code_info.argtypes = [ip, cp, ctypes.POINTER(LdpcInfo)]
+        L.drx_ldpc_code_info.restype = ip
+        L.drx_channel_generate.argtypes = [vp, cp, cp, ip, ctypes.c_float, ctypes.c_ulonglong, vp, sz,
+                                           vp, sz, vp, sz, vp]
+        L.drx_channel_generate.restype = ip
+        L.drx_ldpc_device_error.argtypes = [vp]
+        L.drx_ldpc_device_error.restype = ip
+        _lib = L
+    return _lib
+
+
+def last_error():
+    return lib().drx_ldpc_last_error().decode()
+
+
+def fec_lookup(short_frame, rate):
+    """``drx_fec_lookup``: FecParams of a rate string; KeyError if unknown."""
+    p = FecParams()
+    if lib().drx_fec_lookup(int(bool(short_frame)), rate.encode(), ctypes.byref(p)) != 0:
+        raise KeyError(rate)
+    return p
+
+
+def lanes():
+    """``drx_ldpc_lanes``: most frames per ``Ldpc.decode`` call (64)."""
+    return lib().drx_ldpc_lanes()
+
+
+def code_info(short_frame, rate):
+    """``drx_ldpc_code_info``: geometry of a code, computed on the host."""
+    info = LdpcInfo()
+    if lib().drx_ldpc_code_info(int(bool(short_frame)), rate.encode(), ctypes.byref(info)) != 0:
+        raise KeyError(rate)
+    return info
+
+
+def _ptrs(rows):
+    arr = (ctypes.c_void_p * len(rows))()
+    for i, r in enumerate(rows):
+        arr[i] = r.ctypes.data
+    return arr
+
+
+class Ldpc:
+    """A decoder handle for one code (``drx_ldpc_new`` / ``drx_ldpc_free``)."""
+
+    def __init__(self, params, rate):
+        self._lib = lib()
+        self.rate = rate
+        self.params = FecParams(params.short_frame, params.nldpc, params.kldpc, params.kbch, params.t)
+        self.h = self._lib.drx_ldpc_new(ctypes.byref(self.params), rate.encode())
+        if not self.h:
+            raise RuntimeError("drx_ldpc_new(%s): %s" % (rate, last_error()))
+        info = LdpcInfo()
+        self._lib.drx_ldpc_get_info(self.h, ctypes.byref(info))
+        self.info = info
+        self.N = info.nldpc
+        self.kldpc = info.kldpc
+        self.nbytes = (info.kldpc + 7) // 8
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.drx_ldpc_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def decode(self, llr, out, max_iter):
+        """``drx_ldpc_decode``: llr and out are sequences of per-frame numpy
+        arrays (int8, nldpc) and (uint8, ceil(kldpc/8)); returns the
+        iterations run or -1."""
+        n = len(llr)
+        for r in llr:
+            assert r.dtype == np.int8 and r.flags.c_contiguous and r.size >= self.N
+        for r in out:
+            assert r.dtype == np.uint8 and r.flags.c_contiguous and r.size >= self.nbytes
+        return self._lib.drx_ldpc_decode(self.h, _ptrs(list(llr)), _ptrs(list(out)), n, int(max_iter))
+
+    def decode_host(self, llr, max_iter, stop=STOP_FRAME):
+        """Host batch: llr [n, nldpc] int8 -> (bits [n, nbytes], iters, ok)."""
+        llr = np.ascontiguousarray(llr, dtype=np.int8)
+        n = llr.shape[0]
+        out = np.zeros((n, self.nbytes), np.uint8)
+        it = np.zeros(n, np.int32)
+        ok = np.zeros(n, np.uint8)
+        r = self._lib.drx_ldpc_decode_host(self.h, llr.ctypes.data, out.ctypes.data, it.ctypes.data,
+                                           ok.ctypes.data, n, int(max_iter), int(stop))
+        if r != 0:
+            raise RuntimeError("drx_ldpc_decode_host: " + last_error())
+        return out, it, ok
+
+    def decode_device(self, llr, max_iter, stop=STOP_FRAME, out=None, iters=None, ok=None, stream=None):
+        """Device batch on torch CUDA tensors (asynchronous on ``stream``,
+        default the current torch stream): llr [n, stride >= nldpc] int8."""
+        import torch
+
+        assert llr.is_cuda and llr.dtype == torch.int8 and llr.dim() == 2 and llr.stride(1) == 1
+        n = llr.shape[0]
+        dev = llr.device
+        if out is None:
+            out = torch.empty((n, self.nbytes), dtype=torch.uint8, device=dev)
+        if iters is None:
+            iters = torch.empty(n, dtype=torch.int32, device=dev)
+        if ok is None:
+            ok = torch.empty(n, dtype=torch.uint8, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        r = self._lib.drx_ldpc_decode_device(
+            self.h, llr.data_ptr(), llr.stride(0), out.data_ptr(), out.stride(0), iters.data_ptr(),
+            ok.data_ptr(), n, int(max_iter), int(stop), ctypes.c_void_p(s.cuda_stream))
+        if r != 0:
+            raise RuntimeError("drx_ldpc_decode_device: " + last_error())
+        return out, iters, ok
+
+    def generate(self, nframes, esn0_db, seed, constellation="QPSK", const_rate=None, llr=True,
+                 info=False, llr_f16=False, stream=None):
+        """``drx_channel_generate``: seeded synthetic frames of this code on
+        the GPU.  Returns (llr int8 [n, N] or None, info uint8 [n, nbytes] or
+        None, llr_f16 float16 [n, N] or None) as torch CUDA tensors."""
+        import torch
+
+        dev = torch.device("cuda", torch.cuda.current_device())
+        t_llr = torch.empty((nframes, self.N), dtype=torch.int8, device=dev) if llr else None
+        t_info = torch.empty((nframes, self.nbytes), dtype=torch.uint8, device=dev) if info else None
+        t_h = torch.empty((nframes, self.N), dtype=torch.float16, device=dev) if llr_f16 else None
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        r = self._lib.drx_channel_generate(
+            self.h, constellation.encode(), (const_rate or self.rate).encode(), int(nframes),
+            ctypes.c_float(esn0_db), ctypes.c_ulonglong(seed),
+            t_llr.data_ptr() if t_llr is not None else None, self.N,
+            t_h.data_ptr() if t_h is not None else None, self.N,
+            t_info.data_ptr() if t_info is not None else None, self.nbytes,
+            ctypes.c_void_p(s.cuda_stream))
+        if r != 0:
+            raise RuntimeError("drx_channel_generate: " + last_error())
+        return t_llr, t_info, t_h
+
+    def device_error(self):
+        return self._lib.drx_ldpc_device_error(self.h)

@@ -1,0 +1,538 @@
+/*
+ * extern "C" entry points of libdvbrx_b200.so (declared in include/dvbrx_b200.h).
+ *
+ * A handle holds one compiled code (its tables in device memory), a CUDA
+ * stream, the per-CTA message scratch, the group-barrier counters and the
+ * pinned staging buffers of the host-pointer calls.
+ */
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dvbrx_b200.h"
+#include <math.h>
+
+#include "channel.h"
+#include "codes.h"
+#include "codes_gen.h"
+#include "ldpc_device.h"
+
+using namespace drxg;
+
+namespace {
+
+thread_local std::string g_err;
+
+void set_err(const std::string& s) { g_err = s; }
+
+bool cuda_ok(cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess)
+        return true;
+    set_err(std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+constexpr int kLanes = 64;
+
+}  // namespace
+
+struct drx_ldpc {
+    int device = 0;
+    int sms = 0;
+    Code code;
+    drx_fec_params params{};
+    int nbytes = 0;
+    void* blob = nullptr; /* device: DevCode + tables */
+    DevCode* dcode = nullptr;
+    size_t smem = 0;
+    int ctas_per_sm = 0;
+    cudaStream_t stream = nullptr;
+    /* scratch */
+    void* msg = nullptr;
+    size_t msg_cap = 0;
+    unsigned* work = nullptr;
+    unsigned* sync = nullptr;
+    size_t sync_cap = 0;
+    int* err = nullptr;
+    /* staging of the host-pointer calls */
+    int8_t* h_llr = nullptr;
+    uint8_t* h_out = nullptr;
+    int32_t* h_it = nullptr;
+    uint8_t* h_ok = nullptr;
+    int8_t* d_llr = nullptr;
+    uint8_t* d_out = nullptr;
+    int32_t* d_it = nullptr;
+    uint8_t* d_ok = nullptr;
+    size_t stage_frames = 0;
+};
+
+namespace {
+
+void release_stage(drx_ldpc* d)
+{
+    cudaFreeHost(d->h_llr);
+    cudaFreeHost(d->h_out);
+    cudaFreeHost(d->h_it);
+    cudaFreeHost(d->h_ok);
+    cudaFree(d->d_llr);
+    cudaFree(d->d_out);
+    cudaFree(d->d_it);
+    cudaFree(d->d_ok);
+    d->h_llr = nullptr;
+    d->h_out = nullptr;
+    d->h_it = nullptr;
+    d->h_ok = nullptr;
+    d->d_llr = nullptr;
+    d->d_out = nullptr;
+    d->d_it = nullptr;
+    d->d_ok = nullptr;
+    d->stage_frames = 0;
+}
+
+bool ensure_stage(drx_ldpc* d, size_t nframes)
+{
+    if (d->stage_frames >= nframes)
+        return true;
+    cudaStreamSynchronize(d->stream);
+    release_stage(d);
+    const size_t N = d->code.N, nb = d->nbytes;
+    if (!cuda_ok(cudaMallocHost(&d->h_llr, nframes * N), "cudaMallocHost") ||
+        !cuda_ok(cudaMallocHost(&d->h_out, nframes * nb), "cudaMallocHost") ||
+        !cuda_ok(cudaMallocHost(&d->h_it, nframes * 4), "cudaMallocHost") ||
+        !cuda_ok(cudaMallocHost(&d->h_ok, nframes), "cudaMallocHost") ||
+        !cuda_ok(cudaMalloc(&d->d_llr, nframes * N), "cudaMalloc") ||
+        !cuda_ok(cudaMalloc(&d->d_out, nframes * nb), "cudaMalloc") ||
+        !cuda_ok(cudaMalloc(&d->d_it, nframes * 4), "cudaMalloc") ||
+        !cuda_ok(cudaMalloc(&d->d_ok, nframes), "cudaMalloc")) {
+        release_stage(d);
+        return false;
+    }
+    d->stage_frames = nframes;
+    return true;
+}
+
+bool ensure_msg(drx_ldpc* d, int grid)
+{
+    const size_t need = decode_msg_bytes(d->code.R, d->code.dclass) * (size_t)grid;
+    if (d->msg_cap >= need)
+        return true;
+    cudaStreamSynchronize(d->stream);
+    cudaFree(d->msg);
+    d->msg = nullptr;
+    d->msg_cap = 0;
+    if (!cuda_ok(cudaMalloc(&d->msg, need), "cudaMalloc(messages)"))
+        return false;
+    d->msg_cap = need;
+    return true;
+}
+
+bool ensure_sync(drx_ldpc* d, size_t words)
+{
+    if (d->sync_cap >= words)
+        return true;
+    cudaStreamSynchronize(d->stream);
+    cudaFree(d->sync);
+    d->sync = nullptr;
+    d->sync_cap = 0;
+    if (!cuda_ok(cudaMalloc(&d->sync, words * sizeof(unsigned)), "cudaMalloc(sync)"))
+        return false;
+    d->sync_cap = words;
+    return true;
+}
+
+/* Upload a compiled code: DevCode, then its tables. */
+bool upload_code(drx_ldpc* d)
+{
+    const Code& c = d->code;
+    auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+    const size_t o_ent = a16(sizeof(DevCode));
+    const size_t o_eoff = o_ent + a16(c.ent.size() * sizeof(int32_t));
+    const size_t o_steps = o_eoff + a16(c.eoff.size() * sizeof(uint16_t));
+    const size_t o_perm = o_steps + a16(c.steps.size() * sizeof(uint32_t));
+    const size_t total = o_perm + a16(c.perm.size() * sizeof(uint16_t));
+    std::vector<char> host(total, 0);
+    if (!cuda_ok(cudaMalloc(&d->blob, total), "cudaMalloc(code)"))
+        return false;
+    char* base = (char*)d->blob;
+    DevCode dc{};
+    dc.N = c.N;
+    dc.K = c.K;
+    dc.R = c.R;
+    dc.q = c.q;
+    dc.kldpc = d->params.kldpc;
+    dc.nbytes = d->nbytes;
+    dc.nent = (int)c.ent.size() / 2;
+    dc.nsteps = (int)c.steps.size();
+    dc.dclass = c.dclass;
+    dc.ent = (const int2*)(base + o_ent);
+    dc.eoff = (const uint16_t*)(base + o_eoff);
+    dc.steps = (const uint32_t*)(base + o_steps);
+    dc.perm = (const uint16_t*)(base + o_perm);
+    memcpy(host.data(), &dc, sizeof(dc));
+    memcpy(host.data() + o_ent, c.ent.data(), c.ent.size() * sizeof(int32_t));
+    memcpy(host.data() + o_eoff, c.eoff.data(), c.eoff.size() * sizeof(uint16_t));
+    memcpy(host.data() + o_steps, c.steps.data(), c.steps.size() * sizeof(uint32_t));
+    memcpy(host.data() + o_perm, c.perm.data(), c.perm.size() * sizeof(uint16_t));
+    if (!cuda_ok(cudaMemcpy(d->blob, host.data(), total, cudaMemcpyHostToDevice), "cudaMemcpy(code)"))
+        return false;
+    d->dcode = (DevCode*)d->blob;
+    d->smem = decode_smem_bytes(c.N, dc.nent, dc.nsteps, c.q);
+    return true;
+}
+
+/* Queue one decode of nframes device-resident frames. */
+int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, size_t out_stride,
+            int32_t* iters, uint8_t* ok, int nframes, int max_iter, int stop, cudaStream_t s)
+{
+    if (nframes <= 0)
+        return 0;
+    if (max_iter < 0) /* the reference's loop runs no iteration then (ldpc.c:628) */
+        max_iter = 0;
+    if (stop < 0) {
+        set_err("stop must be DRX_STOP_FRAME or a group size > 0");
+        return -1;
+    }
+    if (llr_stride < (size_t)d->code.N || out_stride < (size_t)d->nbytes) {
+        set_err("row stride below the frame size");
+        return -1;
+    }
+    const int capacity = d->ctas_per_sm * d->sms;
+    if (capacity <= 0) {
+        set_err("decoder kernel cannot be resident on this device");
+        return -1;
+    }
+    DecodeParams p{};
+    p.code = d->dcode;
+    p.llr = llr;
+    p.llr_stride = llr_stride;
+    p.out = out;
+    p.out_stride = out_stride;
+    p.iters = iters;
+    p.ok = ok;
+    p.nframes = nframes;
+    p.max_iter = max_iter;
+    p.err = d->err;
+    int grid;
+    if (stop == 0) {
+        grid = std::min(nframes, capacity);
+        p.group = 0;
+        p.work = d->work;
+        if (!cuda_ok(cudaMemsetAsync(d->work, 0, sizeof(unsigned), s), "cudaMemsetAsync"))
+            return -1;
+    } else {
+        const int G = stop;
+        if (G > capacity) {
+            set_err("group larger than the resident CTAs of this device");
+            return -1;
+        }
+        const int ngroups = (nframes + G - 1) / G;
+        const int nteams = std::min(ngroups, capacity / G);
+        const int per_team = (ngroups + nteams - 1) / nteams;
+        const size_t words = 2 * (size_t)(std::max(max_iter, 0) + 1) * (size_t)nteams * per_team;
+        if (!ensure_sync(d, words))
+            return -1;
+        if (!cuda_ok(cudaMemsetAsync(d->sync, 0, words * sizeof(unsigned), s), "cudaMemsetAsync"))
+            return -1;
+        grid = nteams * G;
+        p.group = G;
+        p.nteams = nteams;
+        p.team_sync = d->sync;
+    }
+    if (!ensure_msg(d, grid))
+        return -1;
+    p.msg = d->msg;
+    p.msg_stride = decode_msg_bytes(d->code.R, d->code.dclass);
+    return cuda_ok(launch_decode(p, d->code.dclass, d->smem, grid, s), "decoder launch") ? 0 : -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* drx_ldpc_last_error(void) { return g_err.c_str(); }
+
+int drx_fec_lookup(int short_frame, const char* rate, drx_fec_params* p)
+{
+    if (!rate || !p)
+        return -1;
+    const cg_fec* rows = short_frame ? cg_fec_short : cg_fec_normal;
+    const int n = short_frame ? (int)(sizeof(cg_fec_short) / sizeof(*cg_fec_short))
+                              : (int)(sizeof(cg_fec_normal) / sizeof(*cg_fec_normal));
+    for (int i = 0; i < n; i++) {
+        if (strcmp(rows[i].rate, rate) == 0) {
+            p->short_frame = short_frame;
+            p->nldpc = short_frame ? 16200 : 64800;
+            p->kldpc = rows[i].nbch;
+            p->kbch = rows[i].kbch;
+            p->t = rows[i].t;
+            return 0;
+        }
+    }
+    return -1;
+}
+
+int drx_ldpc_lanes(void) { return kLanes; }
+
+drx_ldpc* drx_ldpc_new(const drx_fec_params* p, const char* rate)
+{
+    if (!p || !rate) {
+        set_err("NULL argument");
+        return nullptr;
+    }
+    const int table = find_table(p->short_frame, rate);
+    if (table < 0) {
+        set_err(std::string("no LDPC table for rate ") + rate);
+        return nullptr;
+    }
+    drx_ldpc* d = new drx_ldpc();
+    std::string err;
+    if (!compile_code(table, &d->code, &err)) {
+        set_err(err);
+        delete d;
+        return nullptr;
+    }
+    d->params = *p;
+    if (d->params.kldpc <= 0 || d->params.kldpc > d->code.K)
+        d->params.kldpc = d->code.K;
+    d->nbytes = (d->params.kldpc + 7) / 8;
+    if (!cuda_ok(cudaGetDevice(&d->device), "cudaGetDevice") ||
+        !cuda_ok(cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount, d->device),
+                 "cudaDeviceGetAttribute") ||
+        !cuda_ok(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "cudaStreamCreate") ||
+        !upload_code(d) || !cuda_ok(cudaMalloc(&d->work, 256), "cudaMalloc") ||
+        !cuda_ok(cudaMalloc(&d->err, sizeof(int)), "cudaMalloc") ||
+        !cuda_ok(cudaMemset(d->err, 0, sizeof(int)), "cudaMemset")) {
+        drx_ldpc_free(d);
+        return nullptr;
+    }
+    d->ctas_per_sm = decode_ctas_per_sm(d->code.dclass, d->smem);
+    if (d->ctas_per_sm <= 0) {
+        set_err("decoder kernel does not fit on this device");
+        drx_ldpc_free(d);
+        return nullptr;
+    }
+    return d;
+}
+
+void drx_ldpc_free(drx_ldpc* d)
+{
+    if (!d)
+        return;
+    if (d->stream)
+        cudaStreamSynchronize(d->stream);
+    release_stage(d);
+    cudaFree(d->msg);
+    cudaFree(d->sync);
+    cudaFree(d->work);
+    cudaFree(d->err);
+    cudaFree(d->blob);
+    if (d->stream)
+        cudaStreamDestroy(d->stream);
+    delete d;
+}
+
+int drx_ldpc_get_info(const drx_ldpc* d, drx_ldpc_info* info)
+{
+    if (!d || !info)
+        return -1;
+    info->nldpc = d->code.N;
+    info->kldpc = d->params.kldpc;
+    info->K = d->code.K;
+    info->R = d->code.R;
+    info->q = d->code.q;
+    info->edges = d->code.edges;
+    info->steps = (int)d->code.steps.size();
+    info->deg_max = d->code.deg_max;
+    info->levelled = d->code.levelled ? 1 : 0;
+    return 0;
+}
+
+int drx_ldpc_code_info(int short_frame, const char* rate, drx_ldpc_info* info)
+{
+    if (!rate || !info)
+        return -1;
+    const int table = find_table(short_frame, rate);
+    if (table < 0) {
+        set_err(std::string("no LDPC table for rate ") + rate);
+        return -1;
+    }
+    Code c;
+    std::string err;
+    if (!compile_code(table, &c, &err)) {
+        set_err(err);
+        return -1;
+    }
+    drx_fec_params p{};
+    info->kldpc = drx_fec_lookup(short_frame, rate, &p) == 0 ? p.kldpc : c.K;
+    info->nldpc = c.N;
+    info->K = c.K;
+    info->R = c.R;
+    info->q = c.q;
+    info->edges = c.edges;
+    info->steps = (int)c.steps.size();
+    info->deg_max = c.deg_max;
+    info->levelled = c.levelled ? 1 : 0;
+    return 0;
+}
+
+int drx_ldpc_device_error(drx_ldpc* d)
+{
+    if (!d)
+        return -1;
+    int v = 0;
+    cudaStreamSynchronize(d->stream);
+    cudaMemcpy(&v, d->err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemset(d->err, 0, sizeof(int));
+    return v;
+}
+
+int drx_ldpc_decode_device(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out,
+                           size_t out_stride, int32_t* iters, uint8_t* ok, int nframes,
+                           int max_iter, int stop, void* stream)
+{
+    if (!d || (nframes > 0 && (!llr || !out))) {
+        set_err("NULL argument");
+        return -1;
+    }
+    return enqueue(d, llr, llr_stride, out, out_stride, iters, ok, nframes, max_iter, stop,
+                   stream ? (cudaStream_t)stream : d->stream);
+}
+
+int drx_ldpc_decode_host(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t* iters,
+                         uint8_t* ok, int nframes, int max_iter, int stop)
+{
+    if (!d || (nframes > 0 && (!llr || !out))) {
+        set_err("NULL argument");
+        return -1;
+    }
+    if (nframes <= 0)
+        return 0;
+    const size_t N = d->code.N, nb = d->nbytes;
+    cudaStream_t s = d->stream;
+    if (!ensure_stage(d, nframes))
+        return -1;
+    memcpy(d->h_llr, llr, (size_t)nframes * N);
+    if (!cuda_ok(cudaMemcpyAsync(d->d_llr, d->h_llr, (size_t)nframes * N, cudaMemcpyHostToDevice, s),
+                 "cudaMemcpyAsync"))
+        return -1;
+    if (enqueue(d, d->d_llr, N, d->d_out, nb, d->d_it, d->d_ok, nframes, max_iter, stop, s))
+        return -1;
+    if (!cuda_ok(cudaMemcpyAsync(d->h_out, d->d_out, (size_t)nframes * nb, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync") ||
+        !cuda_ok(cudaMemcpyAsync(d->h_it, d->d_it, (size_t)nframes * 4, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync") ||
+        !cuda_ok(cudaMemcpyAsync(d->h_ok, d->d_ok, (size_t)nframes, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync") ||
+        !cuda_ok(cudaStreamSynchronize(s), "decode"))
+        return -1;
+    memcpy(out, d->h_out, (size_t)nframes * nb);
+    if (iters)
+        memcpy(iters, d->h_it, (size_t)nframes * 4);
+    if (ok)
+        memcpy(ok, d->h_ok, (size_t)nframes);
+    return 0;
+}
+
+int drx_channel_generate(drx_ldpc* d, const char* constellation, const char* const_rate, int nframes,
+                         float esn0_db, unsigned long long seed, int8_t* llr, size_t llr_stride,
+                         void* llr_f16, size_t llr_f16_stride, uint8_t* info, size_t info_stride,
+                         void* stream)
+{
+    if (!d || !constellation || !const_rate) {
+        set_err("NULL argument");
+        return -1;
+    }
+    if (nframes <= 0)
+        return 0;
+    const int short_frame = d->code.N == 16200 ? 1 : 0;
+    const cg_const* row = nullptr;
+    for (int i = 0; i < CG_NCONSTS; i++)
+        if (!strcmp(cg_consts[i].name, constellation) && !strcmp(cg_consts[i].rate, const_rate) &&
+            cg_consts[i].short_frame == short_frame)
+            row = &cg_consts[i];
+    if (!row) {
+        set_err(std::string("no constellation ") + constellation + " " + const_rate);
+        return -1;
+    }
+    if ((llr && llr_stride < (size_t)d->code.N) || (llr_f16 && llr_f16_stride < (size_t)d->code.N) ||
+        (info && info_stride < (size_t)d->nbytes)) {
+        set_err("row stride below the frame size");
+        return -1;
+    }
+    ChannelParams p{};
+    p.code = d->dcode;
+    p.seed = seed;
+    p.n0 = powf(10.0f, -esn0_db / 10.0f);
+    p.bits = row->bits;
+    p.qpsk = row->order[0] < 0;
+    const int np = 1 << row->bits;
+    double e = 0;
+    for (int i = 0; i < np; i++)
+        e += (double)row->points[2 * i] * row->points[2 * i] + (double)row->points[2 * i + 1] * row->points[2 * i + 1];
+    const float g = (float)(1.0 / sqrt(e / np)); /* unit average energy, as demap.c:183-187 */
+    for (int i = 0; i < np; i++) {
+        p.re[i] = row->points[2 * i] * g;
+        p.im[i] = row->points[2 * i + 1] * g;
+        p.e[i] = p.re[i] * p.re[i] + p.im[i] * p.im[i];
+    }
+    for (int b = 0; b < 8; b++)
+        p.order[b] = row->order[b] < 0 ? 0 : row->order[b];
+    p.llr = llr;
+    p.llr_stride = llr_stride;
+    p.llr_f16 = (__half*)llr_f16;
+    p.llr_f16_stride = llr_f16_stride;
+    p.info = info;
+    p.info_stride = info_stride;
+    return cuda_ok(launch_channel(p, nframes, d->code.N, stream ? (cudaStream_t)stream : d->stream),
+                   "channel launch") ? 0 : -1;
+}
+
+int drx_ldpc_decode(drx_ldpc* d, const int8_t* const* llr, uint8_t* const* out, int nframes,
+                    int max_iter)
+{
+    if (!d) {
+        set_err("NULL handle");
+        return -1;
+    }
+    if (nframes > kLanes) /* ldpc.c:620-621 */
+        return -1;
+    if (nframes <= 0) /* every lane padded: the syndrome passes at once */
+        return 0;
+    if (!llr || !out) {
+        set_err("NULL argument");
+        return -1;
+    }
+    const size_t N = d->code.N, nb = d->nbytes;
+    cudaStream_t s = d->stream;
+    if (!ensure_stage(d, kLanes))
+        return -1;
+    for (int f = 0; f < nframes; f++)
+        memcpy(d->h_llr + (size_t)f * N, llr[f], N);
+    if (!cuda_ok(cudaMemcpyAsync(d->d_llr, d->h_llr, (size_t)nframes * N, cudaMemcpyHostToDevice, s),
+                 "cudaMemcpyAsync"))
+        return -1;
+    if (enqueue(d, d->d_llr, N, d->d_out, nb, d->d_it, d->d_ok, nframes, max_iter, nframes, s))
+        return -1;
+    if (!cuda_ok(cudaMemcpyAsync(d->h_out, d->d_out, (size_t)nframes * nb, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync") ||
+        !cuda_ok(cudaMemcpyAsync(d->h_it, d->d_it, (size_t)nframes * 4, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync") ||
+        !cuda_ok(cudaMemcpyAsync(d->h_ok, d->d_ok, (size_t)nframes, cudaMemcpyDeviceToHost, s),
+                 "cudaMemcpyAsync") ||
+        !cuda_ok(cudaStreamSynchronize(s), "decode"))
+        return -1;
+    for (int f = 0; f < nframes; f++)
+        memcpy(out[f], d->h_out + (size_t)f * nb, nb);
+    int all = 1;
+    for (int f = 0; f < nframes; f++)
+        all &= d->h_ok[f];
+    return all ? d->h_it[0] : -1;
+}
+
+}  // extern "C"

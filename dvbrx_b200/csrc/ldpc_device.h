@@ -1,0 +1,58 @@
+/*
+ * Device-side code descriptor and the launchers of the plain decoder.
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace drxg {
+
+constexpr int kThreads = 384; /* 360 checks of a layer, 12 warps */
+
+/* One code as the kernels read it (device memory). */
+struct DevCode {
+    int N, K, R, q, kldpc, nbytes;
+    int nent, nsteps, dclass;
+    int pad;
+    const int2* ent;       /* nent pairs (360 g - a, a), layer-major */
+    const uint16_t* eoff;  /* q + 1 */
+    const uint32_t* steps; /* nsteps: layer | start << 8 | count << 17 | perm << 26 */
+    const uint16_t* perm;  /* q * 360 */
+};
+
+/* Work of one launch of the plain decoder. */
+struct DecodeParams {
+    const DevCode* code;   /* device pointer */
+    const int8_t* llr;     /* nframes rows of llr_stride bytes (N used) */
+    size_t llr_stride;
+    uint8_t* out;          /* nframes rows of out_stride bytes (nbytes used) */
+    size_t out_stride;
+    int32_t* iters;        /* nframes, may be null */
+    uint8_t* ok;           /* nframes, may be null */
+    int nframes;
+    int max_iter;
+    int group;             /* 0: each frame stops on its own; G > 0: groups of G
+                              consecutive frames stop together (reference
+                              batch semantics), launched cooperatively */
+    int nteams;            /* group mode: grid / group */
+    unsigned* work;        /* per-frame mode: frame counter, zeroed by the launcher */
+    unsigned* team_sync;   /* group mode: 2 * nteams * groups_per_team * (max_iter + 1) */
+    void* msg;             /* message scratch: grid * msg_stride bytes */
+    size_t msg_stride;
+    int* err;              /* device error word (0 = fine) */
+};
+
+/* Largest dynamic shared memory of the plain kernel for a code. */
+size_t decode_smem_bytes(int N, int nent, int nsteps, int q);
+/* Message scratch per CTA. */
+size_t decode_msg_bytes(int R, int dclass);
+/* Resident CTAs per SM of the plain kernel for a class and smem size. */
+int decode_ctas_per_sm(int dclass, size_t smem);
+
+/* Launch the plain decoder on `grid` CTAs.  Group mode uses a cooperative
+ * launch (co-resident CTAs are required by the group barrier). */
+cudaError_t launch_decode(const DecodeParams& p, int dclass, size_t smem, int grid,
+                          cudaStream_t stream);
+
+}  // namespace drxg

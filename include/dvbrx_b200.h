@@ -1,0 +1,129 @@
+/*
+ * dvbrx_b200: DVB-S2 / S2X / T2 LDPC decoding on an NVIDIA B200 (sm_100a).
+ *
+ * C ABI of libdvbrx_b200.so.  The first five entry points are the drop-in
+ * for the reference receiver's decoder (TrusterBSW/DVB-Rx, libdvbrx): same
+ * names, same argument meaning, same return values.  A program built against
+ * libdvbrx's ldpc.h and fec.h links against this library unchanged.  The
+ * rest are additions for batches that do not fit the reference's 64-lane
+ * call: device-resident batches, mixed-code batches and the learned decoder.
+ *
+ * Plain pointers and sizes only; `stream` arguments are cudaStream_t values
+ * passed as void* (NULL: the handle's own stream).
+ */
+#ifndef DVBRX_B200_H
+#define DVBRX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- drop-in: reference libdvbrx/include/dvbrx/fec.h, ldpc.h ------------ */
+
+/* Same layout as the reference's drx_fec_params (libdvbrx/include/dvbrx/fec.h:13-19). */
+#ifndef DVBRX_FEC_H
+typedef struct {
+    int short_frame; /* 0: normal (64800 bits), 1: short (16200 bits) */
+    int nldpc;       /* LDPC codeword length */
+    int kldpc;       /* = nbch */
+    int kbch;        /* BBFRAME length */
+    int t;           /* BCH error-correcting capability */
+} drx_fec_params;
+#endif
+
+typedef struct drx_ldpc drx_ldpc;
+
+/* Replaces drx_fec_lookup (libdvbrx/include/dvbrx/fec.h:25, libdvbrx/src/bch.c:25-41):
+ * FEC parameters of a rate string ("3_4", "13_45", "1_5_VLSNR_SF2", ...).
+ * Returns 0 on success, -1 for an unknown rate. */
+int drx_fec_lookup(int short_frame, const char* rate, drx_fec_params* p);
+
+/* Replaces drx_ldpc_lanes (libdvbrx/include/dvbrx/ldpc.h:17, ldpc.c:186): the most
+ * frames one drx_ldpc_decode call takes.  64, the size callers give their
+ * pointer arrays (libdvbrx/src/rx.c:14, rxmt.c:23). */
+int drx_ldpc_lanes(void);
+
+/* Replaces drx_ldpc_new (libdvbrx/include/dvbrx/ldpc.h:20, ldpc.c:199-260).  Returns
+ * NULL for an unknown rate or when no CUDA device or memory is available
+ * (drx_ldpc_last_error() says which).  The handle owns its GPU memory and
+ * stream; like the reference's, it is not thread-safe. */
+drx_ldpc* drx_ldpc_new(const drx_fec_params* p, const char* rate);
+
+/* Replaces drx_ldpc_free (libdvbrx/include/dvbrx/ldpc.h:21, ldpc.c:262-273); NULL-safe. */
+void drx_ldpc_free(drx_ldpc* d);
+
+/* Replaces drx_ldpc_decode (libdvbrx/include/dvbrx/ldpc.h:32-36, ldpc.c:614-638).
+ * llr[f]: nldpc int8 LLRs of frame f (host memory, positive for a 0 bit);
+ * out[f]: receives ceil(kldpc / 8) bytes of hard information bits, MSB first.
+ * The frames are decoded together with the reference's semantics: they
+ * iterate until all pass the syndrome check or max_iter is reached.  Returns
+ * the iterations run, or -1 if some frame still fails (hard bits are written
+ * either way), or if nframes > drx_ldpc_lanes().  Synchronous. */
+int drx_ldpc_decode(drx_ldpc* d, const int8_t* const* llr, uint8_t* const* out, int nframes,
+                    int max_iter);
+
+/* ---- additions ---------------------------------------------------------- */
+
+/* Message of the last failure in this thread ("" if none). */
+const char* drx_ldpc_last_error(void);
+
+/* Code geometry of a handle. */
+typedef struct {
+    int nldpc, kldpc, K, R, q;
+    int edges;    /* links of the Tanner graph */
+    int steps;    /* layer steps per iteration (wavefront levels) */
+    int deg_max;  /* largest check degree */
+    int levelled; /* some layer needs more than one step */
+} drx_ldpc_info;
+int drx_ldpc_get_info(const drx_ldpc* d, drx_ldpc_info* info);
+
+/* The same geometry for a rate, computed on the host (no device needed);
+ * kldpc is taken from the BCH table, or K for codes without one.
+ * Returns 0, or -1 for an unknown rate. */
+int drx_ldpc_code_info(int short_frame, const char* rate, drx_ldpc_info* info);
+
+/* Stopping rule of the batch calls: DRX_STOP_FRAME stops every frame on its
+ * own (its iteration count and flag are those of a one-frame
+ * drx_ldpc_decode call); a value G > 0 stops groups of G consecutive
+ * frames together, as a drx_ldpc_decode call with those G frames would. */
+#define DRX_STOP_FRAME 0
+
+/* Decode nframes frames already in device memory, asynchronously on
+ * `stream`.  llr: frame f at llr + f * llr_stride (nldpc bytes used);
+ * out: frame f at out + f * out_stride (ceil(kldpc/8) bytes); iters, ok:
+ * nframes entries each, or NULL.  Returns 0 if the work was queued. */
+int drx_ldpc_decode_device(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out,
+                           size_t out_stride, int32_t* iters, uint8_t* ok, int nframes,
+                           int max_iter, int stop, void* stream);
+
+/* The same with host buffers (contiguous rows), synchronous: stages through
+ * pinned memory and returns 0 when the results are in place. */
+int drx_ldpc_decode_host(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t* iters,
+                         uint8_t* ok, int nframes, int max_iter, int stop);
+
+/* Seeded synthetic frames of the handle's code, in device memory: random
+ * information bits (Philox4x32-10 keyed by seed and frame index), the DVB-S2
+ * encoder, the bit interleaver and constellation of the MODCOD
+ * (constellation "QPSK" / "8PSK" / "16APSK" / ..., const_rate the rate row
+ * of that constellation table), complex AWGN at esn0_db and the max-log
+ * demapper with the reference receiver's int8 scale (2 x LLR, saturated to
+ * +-127, libdvbrx/src/demap.c:491-533).  Any of llr (int8 rows), llr_f16
+ * (IEEE half rows of the unquantised values) and info (packed information
+ * bits, kldpc bits MSB first) may be NULL.  Asynchronous on `stream`. */
+int drx_channel_generate(drx_ldpc* d, const char* constellation, const char* const_rate, int nframes,
+                         float esn0_db, unsigned long long seed, int8_t* llr, size_t llr_stride,
+                         void* llr_f16, size_t llr_f16_stride, uint8_t* info, size_t info_stride,
+                         void* stream);
+
+/* Device error word of the handle: 0, or the code of a device-side fault
+ * report (2: a group barrier timed out).  Cleared by the call. */
+int drx_ldpc_device_error(drx_ldpc* d);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DVBRX_B200_H */

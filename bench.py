@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--e2e-steps", type=int, default=7)
+    ap.add_argument("--batches", type=int, default=len(ESN0),
+                    help="Es/N0 points held on the device (small profiling cases use fewer)")
     return ap.parse_args()
 
 
@@ -228,7 +230,8 @@ def run_reference(args):
         "impl": "reference",
         "config": dict(workload_config(lanes * threads, 1),
                        stopping="per batch of %d frames (reference drx_ldpc_decode semantics)" % lanes,
-                       frames_per_step=lanes * threads),
+                       frames_per_step=lanes * threads, l2="n/a (host CPU)",
+                       parallelism="one thread and one decoder handle per host core"),
         "cpu_baseline": {"value": gbps, "unit": UNIT, "cores": threads, "kind": "reference",
                          "lanes": lanes,
                          "sample": "%d steps x %d threads x one %d-frame drx_ldpc_decode call" % (
@@ -264,7 +267,7 @@ def run_b200(args):
 
     # inputs: one batch per Es/N0 point, resident in HBM
     llr, info = [], []
-    for k, es in enumerate(ESN0):
+    for k, es in enumerate(ESN0[: args.batches]):
         l, inf, _ = dec.generate(F, es, seed=1000003 * (rank + 1) + k, constellation=CONST, info=True)
         llr.append(l)
         info.append(inf)
@@ -275,7 +278,7 @@ def run_b200(args):
     torch.cuda.synchronize()
 
     def step(k, it_buf, ok_buf):
-        dec.decode_device(llr[k % len(ESN0)], MAX_ITER, out=out, iters=it_buf, ok=ok_buf)
+        dec.decode_device(llr[k % len(llr)], MAX_ITER, out=out, iters=it_buf, ok=ok_buf)
 
     for k in range(args.warmup):
         step(k, iters[0], oks[0])
@@ -294,7 +297,7 @@ def run_b200(args):
         step(args.warmup + k, iters[k], oks[k])
         ev[k][1].record(stream)
         # frame errors of this step (outside the kernel's events)
-        errs[k] = (out != info[(args.warmup + k) % len(ESN0)]).any(dim=1).sum()
+        errs[k] = (out != info[(args.warmup + k) % len(info)]).any(dim=1).sum()
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launch_ms = [a.elapsed_time(b) for a, b in ev]
@@ -346,7 +349,7 @@ def run_b200(args):
 
     # end to end through the C ABI with host buffers (synchronous call)
     e2e = None
-    if rank == 0 or world > 1:
+    if args.e2e_steps > 0:
         host = [l.cpu().numpy() for l in llr]
         for k in range(min(2, args.e2e_steps)):
             dec.decode_host(host[k % len(host)], MAX_ITER)

@@ -116,6 +116,14 @@ def code_info(short_frame, rate):
     return info
 
 
+def stream_handle(stream):
+    """cudaStream_t of a torch stream as the C ABI takes it: torch's legacy
+    default stream has handle 0, which the C ABI reads as "the handle's own
+    stream", so it is passed as cudaStreamLegacy (1) instead."""
+    h = stream.cuda_stream
+    return ctypes.c_void_p(h if h else 1)
+
+
 def _ptrs(rows):
     arr = (ctypes.c_void_p * len(rows))()
     for i, r in enumerate(rows):
@@ -189,7 +197,7 @@ class Ldpc:
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         r = self._lib.drx_ldpc_decode_device(
             self.h, llr.data_ptr(), llr.stride(0), out.data_ptr(), out.stride(0), iters.data_ptr(),
-            ok.data_ptr(), n, int(max_iter), int(stop), ctypes.c_void_p(s.cuda_stream))
+            ok.data_ptr(), n, int(max_iter), int(stop), stream_handle(s))
         if r != 0:
             raise RuntimeError("drx_ldpc_decode_device: " + last_error())
         return out, iters, ok
@@ -212,7 +220,7 @@ class Ldpc:
             t_llr.data_ptr() if t_llr is not None else None, self.N,
             t_h.data_ptr() if t_h is not None else None, self.N,
             t_info.data_ptr() if t_info is not None else None, self.nbytes,
-            ctypes.c_void_p(s.cuda_stream))
+            stream_handle(s))
         if r != 0:
             raise RuntimeError("drx_channel_generate: " + last_error())
         return t_llr, t_info, t_h

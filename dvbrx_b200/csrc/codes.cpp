@@ -21,6 +21,14 @@ int find_table(int short_frame, const char* rate)
     return -1;
 }
 
+int degree_class(int deg_max)
+{
+    for (int k = 0; k < kNumClasses; k++)
+        if (deg_max <= kClassDeg[k])
+            return k;
+    return -1;
+}
+
 bool compile_code(int table, Code* c, std::string* err)
 {
     if (table < 0 || table >= CG_NTABLES) {
@@ -79,7 +87,7 @@ bool compile_code(int table, Code* c, std::string* err)
         info_links += (int)layer[i].size() * QC;
     }
     c->deg_max = c->cnt_max + 2;
-    c->dclass = c->deg_max <= 8 ? 0 : c->deg_max <= 16 ? 1 : 2;
+    c->dclass = degree_class(c->deg_max);
     if (c->deg_max > 32) {
         *err = "check degree above 32";
         return false;

@@ -34,7 +34,7 @@ struct Code {
     int N = 0, K = 0, R = 0, q = 0;
     int cnt_max = 0;   /* most information links of a check */
     int deg_max = 0;   /* cnt_max + 2 parity links */
-    int dclass = 0;    /* kernel class: 0 (deg <= 8), 1 (<= 16), 2 (<= 32) */
+    int dclass = 0;    /* kernel class: degree_class(deg_max) */
     int edges = 0;     /* links of the whole Tanner graph */
     int nlevels = 0;   /* steps per iteration */
     bool levelled = false;
@@ -52,6 +52,13 @@ struct Code {
     std::vector<uint16_t> addr;
     std::vector<uint32_t> aoff;
 };
+
+/* Kernel classes by largest check degree: each class's kernel is compiled
+ * for degrees up to kClassDeg[class] only, so that its register budget fits
+ * the codes it runs. */
+constexpr int kNumClasses = 6;
+constexpr int kClassDeg[kNumClasses] = { 7, 11, 14, 18, 22, 32 };
+int degree_class(int deg_max);
 
 /* Rate string -> table index (cg_rates_normal / cg_rates_short), or -1.
  * Mirrors find_table(), libdvbrx/src/ldpc.c:188-197. */

@@ -29,10 +29,12 @@
  *   - hard decision bit = posterior < 0 over the first kldpc bits, packed
  *     MSB first (ldpc.c:581-612).
  */
-#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
+#include "codes.h"
 #include "ldpc_device.h"
 
 namespace drxg {
@@ -40,19 +42,11 @@ namespace drxg {
 constexpr int kQC = 360;
 constexpr int kSpinLimit = 1 << 22; /* polls of a group barrier before giving up */
 
+/* One 32-bit word per check up to degree 16 (6 + 6 + 4 bits, 16 signs),
+ * two above (6 + 6 + 5 bits, 32 signs). */
 template <int DMAX>
-struct MsgWord;
-template <>
-struct MsgWord<8> {
-    typedef uint32_t T;
-};
-template <>
-struct MsgWord<16> {
-    typedef uint32_t T;
-};
-template <>
-struct MsgWord<32> {
-    typedef uint2 T;
+struct MsgWord {
+    typedef typename std::conditional<(DMAX > 16), uint2, uint32_t>::type T;
 };
 
 /* meta = min0 (6 bits) | min1 << 6 | index << 12; signs: bit c = link c */
@@ -82,70 +76,92 @@ __device__ __forceinline__ int sat8(int v) { return max(-128, min(127, v)); }
  * bits.  The result of a min-sum node does not depend on the link order, so
  * the parity links go first to sit at fixed register slots.
  */
-template <int DMAX>
-__device__ __forceinline__ void check_node(int8_t* __restrict__ post, const int2* __restrict__ ent,
-                                           int cnt, int K, int q, int i, int j, bool first,
-                                           uint32_t meta, uint32_t sgn, uint32_t& meta_out,
-                                           uint32_t& sgn_out)
+template <int CNT, int IDXMASK>
+__device__ __forceinline__ void check_node_n(int8_t* __restrict__ post, const int2* __restrict__ ent,
+                                             int K, int q, int i, int j, bool first, uint32_t meta,
+                                             uint32_t sgn, uint32_t& meta_out, uint32_t& sgn_out)
 {
-    int addr[DMAX];
-    int x[DMAX];
+    constexpr int D = CNT + 2;
+    int addr[D];
+    int x[D];
     const bool has_pp = (i | j) != 0;
     addr[0] = K + kQC * i + j;
     addr[1] = i ? addr[0] - kQC : K + kQC * (q - 1) + j - 1;
 #pragma unroll
-    for (int c = 2; c < DMAX; c++)
-        if (c - 2 < cnt) {
-            const int2 e = ent[c - 2];
-            addr[c] = e.x + j + (j < e.y ? kQC : 0);
-        }
+    for (int c = 2; c < D; c++) {
+        const int2 e = ent[c - 2];
+        addr[c] = e.x + j + (j < e.y ? kQC : 0);
+    }
 
-    const int idx = (meta >> 12) & (DMAX > 16 ? 31 : 15);
+    const int idx = (meta >> 12) & IDXMASK;
     const int m0 = meta & 63, m1 = (meta >> 6) & 63;
     /* minus the stored message: +m if the message is negative, else -min(m, 31) */
     const int p0 = -min(m0, 31), n0 = m0, p1 = -min(m1, 31), n1 = m1;
 
     int min0 = 255, min1 = 255, sg = 0;
 #pragma unroll
-    for (int c = 0; c < DMAX; c++) {
-        if (c < cnt + 2) {
-            int v;
-            if (c == 1 && !has_pp) {
-                v = 255; /* no link: larger than every |x|, positive */
-            } else {
-                v = post[addr[c]];
-                if (!first) {
-                    const bool s = (sgn >> c) & 1u;
-                    const int nm = c == idx ? (s ? n1 : p1) : (s ? n0 : p0);
-                    v = sat8(v + nm);
-                }
+    for (int c = 0; c < D; c++) {
+        int v;
+        if (c == 1 && !has_pp) {
+            v = 255; /* no link: larger than every |x|, positive */
+        } else {
+            v = post[addr[c]];
+            if (!first) {
+                const bool s = (sgn >> c) & 1u;
+                const int nm = c == idx ? (s ? n1 : p1) : (s ? n0 : p0);
+                v = sat8(v + nm);
             }
-            x[c] = v;
-            const int a = abs(v);
-            min1 = min(min1, max(min0, a));
-            min0 = min(min0, a);
-            sg ^= v;
         }
+        x[c] = v;
+        const int a = abs(v);
+        min1 = min(min1, max(min0, a));
+        min0 = min(min0, a);
+        sg ^= v;
     }
     const int mn0 = max(min(min0, 127) - 1, 0), mn1 = max(min(min1, 127) - 1, 0);
     int nidx = 0;
     uint32_t nsg = 0;
 #pragma unroll
-    for (int c = 0; c < DMAX; c++) {
-        if (c < cnt + 2) {
-            const int v = x[c];
-            const bool eq = abs(v) == min0;
-            const int mag = eq ? mn1 : mn0;
-            const int sm = (sg ^ v) >> 31; /* -1: negative output */
-            const int o = (mag ^ sm) - sm;
-            if (c != 1 || has_pp)
-                post[addr[c]] = (int8_t)sat8(v + o);
-            nidx = eq ? c : nidx;
-            nsg |= (uint32_t)sm & (1u << c);
-        }
+    for (int c = 0; c < D; c++) {
+        const int v = x[c];
+        const bool eq = abs(v) == min0;
+        const int mag = eq ? mn1 : mn0;
+        const int sm = (sg ^ v) >> 31; /* -1: negative output */
+        const int o = (mag ^ sm) - sm;
+        if (c != 1 || has_pp)
+            post[addr[c]] = (int8_t)sat8(v + o);
+        nidx = eq ? c : nidx;
+        nsg |= (uint32_t)sm & (1u << c);
     }
     meta_out = (uint32_t)min(mn0, 32) | (uint32_t)min(mn1, 32) << 6 | (uint32_t)nidx << 12;
     sgn_out = nsg;
+}
+
+/* Dispatch on the layer's information-link count (uniform over the CTA):
+ * every case is fully unrolled, with no predicated-off link slots. */
+template <int DMAX>
+__device__ __forceinline__ void check_node(int8_t* __restrict__ post, const int2* __restrict__ ent,
+                                           int cnt, int K, int q, int i, int j, bool first,
+                                           uint32_t meta, uint32_t sgn, uint32_t& meta_out,
+                                           uint32_t& sgn_out)
+{
+    constexpr int M = DMAX > 16 ? 31 : 15;
+#define DRXG_CASE(n)                                                                           \
+    case n:                                                                                    \
+        if (n + 2 <= DMAX)                                                                     \
+            check_node_n<(n + 2 <= DMAX ? n : 1), M>(post, ent, K, q, i, j, first, meta, sgn, \
+                                                     meta_out, sgn_out);                       \
+        break;
+    switch (cnt) {
+        DRXG_CASE(1) DRXG_CASE(2) DRXG_CASE(3) DRXG_CASE(4) DRXG_CASE(5) DRXG_CASE(6)
+        DRXG_CASE(7) DRXG_CASE(8) DRXG_CASE(9) DRXG_CASE(10) DRXG_CASE(11) DRXG_CASE(12)
+        DRXG_CASE(13) DRXG_CASE(14) DRXG_CASE(15) DRXG_CASE(16) DRXG_CASE(17) DRXG_CASE(18)
+        DRXG_CASE(19) DRXG_CASE(20) DRXG_CASE(21) DRXG_CASE(22) DRXG_CASE(23) DRXG_CASE(24)
+        DRXG_CASE(25) DRXG_CASE(26) DRXG_CASE(27) DRXG_CASE(28) DRXG_CASE(29) DRXG_CASE(30)
+    default:
+        break;
+    }
+#undef DRXG_CASE
 }
 
 /* Shared-memory image of one code plus the frame's posteriors. */
@@ -417,7 +433,10 @@ size_t decode_smem_bytes(int N, int nent, int nsteps, int q)
            a16(sizeof(uint32_t) * nsteps);
 }
 
-size_t decode_msg_bytes(int R, int dclass) { return (size_t)R * (dclass == 2 ? 8 : 4); }
+size_t decode_msg_bytes(int R, int dclass)
+{
+    return (size_t)R * (kClassDeg[dclass < 0 ? kNumClasses - 1 : dclass] > 16 ? 8 : 4);
+}
 
 template <int DMAX, int MINB>
 static const void* kernel_ptr()
@@ -427,13 +446,20 @@ static const void* kernel_ptr()
 
 static const void* kernel_for(int dclass)
 {
+    static_assert(kNumClasses == 6, "one kernel per degree class");
     switch (dclass) {
     case 0:
-        return kernel_ptr<8, 4>();
+        return kernel_ptr<7, 4>();
     case 1:
-        return kernel_ptr<16, 3>();
+        return kernel_ptr<11, 3>();
+    case 2:
+        return kernel_ptr<14, 3>();
+    case 3:
+        return kernel_ptr<18, 2>();
+    case 4:
+        return kernel_ptr<22, 2>();
     default:
-        return kernel_ptr<32, 2>();
+        return kernel_ptr<32, 1>();
     }
 }
 

@@ -9,7 +9,8 @@
  * call: device-resident batches, mixed-code batches and the learned decoder.
  *
  * Plain pointers and sizes only; `stream` arguments are cudaStream_t values
- * passed as void* (NULL: the handle's own stream).
+ * passed as void*.  NULL means the handle's own stream; pass
+ * cudaStreamLegacy ((void*)1) for the legacy default stream.
  */
 #ifndef DVBRX_B200_H
 #define DVBRX_B200_H

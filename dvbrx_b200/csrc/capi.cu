@@ -536,3 +536,23 @@ int drx_ldpc_decode(drx_ldpc* d, const int8_t* const* llr, uint8_t* const* out, 
 }
 
 }  // extern "C"
+
+namespace drxg {
+
+/* Read-only view of a handle for the allocation-free entry point (noalloc.cu). */
+const DevCode* handle_code(const drx_ldpc* d, int* R, int* dclass, int* N, int* nbytes, int* capacity,
+                           size_t* smem, cudaStream_t* stream)
+{
+    *R = d->code.R;
+    *dclass = d->code.dclass;
+    *N = d->code.N;
+    *nbytes = d->nbytes;
+    *capacity = d->ctas_per_sm * d->sms;
+    *smem = d->smem;
+    *stream = d->stream;
+    return d->dcode;
+}
+
+void handle_set_error(const char* msg) { set_err(msg); }
+
+}  // namespace drxg

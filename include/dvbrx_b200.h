@@ -100,6 +100,23 @@ int drx_ldpc_decode_device(drx_ldpc* d, const int8_t* llr, size_t llr_stride, ui
                            size_t out_stride, int32_t* iters, uint8_t* ok, int nframes,
                            int max_iter, int stop, void* stream);
 
+/* No counterpart in the reference.  drx_ldpc_decode_device with per-frame
+ * stopping for callers that must not allocate GPU memory on the decode path
+ * (a real-time receiver thread, where cudaMalloc/cudaFree can stall on a
+ * device-wide synchronisation; a program whose GPU memory belongs to
+ * another allocator): the call allocates nothing.  Its scratch is a 16 MiB
+ * array compiled into the library, held by every GPU that loads it until
+ * exit; at most (16 MiB - 256) / (R * 4 bytes, 8 above check degree 16)
+ * CTAs run (161 for normal 3/5), and a code whose message slab would not
+ * fit is rejected with an error.  All calls share that array: calls whose
+ * kernels overlap on the GPU race and must be serialised by the caller.
+ * The first call on a device looks up the array's device address (set-up)
+ * and must come before any stream capture.  The handle is made by
+ * drx_ldpc_new beforehand.  Returns 0 if the work was queued. */
+int drx_ldpc_decode_device_noalloc(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out,
+                                   size_t out_stride, int32_t* iters, uint8_t* ok, int nframes,
+                                   int max_iter, void* stream);
+
 /* The same with host buffers (contiguous rows), synchronous: stages through
  * pinned memory and returns 0 when the results are in place. */
 int drx_ldpc_decode_host(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t* iters,

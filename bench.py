@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--e2e-steps", type=int, default=7)
+    ap.add_argument("--variant", default="auto", choices=["auto", "frame"],
+                    help="decoder kernel: automatic choice, or the one-frame kernel")
     ap.add_argument("--batches", type=int, default=len(ESN0),
                     help="Es/N0 points held on the device (small profiling cases use fewer)")
     return ap.parse_args()
@@ -261,6 +263,9 @@ def run_b200(args):
 
     p = D.fec_lookup(SHORT, RATE)
     dec = D.Ldpc(p, RATE)
+    variant = dec.set_variant(D.VARIANT_FRAME if args.variant == "frame" else D.VARIANT_AUTO)
+    kernel_name = {D.VARIANT_PAIR: "drxg::k_decode_pair (two frames per CTA, 16x2 SIMD)",
+                   D.VARIANT_FRAME: "drxg::k_decode (one frame per CTA)"}[variant]
     F = args.frames
     kldpc = p.kldpc
     stream = torch.cuda.current_stream()
@@ -330,7 +335,7 @@ def run_b200(args):
     traffic = profiled_traffic()
     roofline = {
         "bound": "smem",
-        "kernel": "k_decode (drxg::k_decode<16,3>)",
+        "kernel": kernel_name,
         "achieved": smem_bytes / kern_s / 1e9,
         "peak": smem_peak,
         "unit": "GB/s",

@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdvbrx_b200.so")
 
 STOP_FRAME = 0  # DRX_STOP_FRAME
+VARIANT_AUTO, VARIANT_FRAME, VARIANT_PAIR = 0, 1, 2  # DRX_VARIANT_*
 
 _lib = None
 
@@ -53,7 +54,7 @@ class LdpcInfo(ctypes.Structure):
 EXPORTS = (
     "drx_fec_lookup", "drx_ldpc_lanes", "drx_ldpc_new", "drx_ldpc_free", "drx_ldpc_decode",
     "drx_ldpc_last_error", "drx_ldpc_get_info", "drx_ldpc_decode_device", "drx_ldpc_decode_host",
-    "drx_ldpc_device_error", "drx_ldpc_code_info", "drx_channel_generate",
+    "drx_ldpc_device_error", "drx_ldpc_code_info", "drx_channel_generate", "drx_ldpc_set_variant",
 )
 
 
@@ -85,6 +86,19 @@ def lib():
         L.drx_channel_generate.argtypes = [vp, cp, cp, ip, ctypes.c_float, ctypes.c_ulonglong, vp, sz,
                                            vp, sz, vp, sz, vp]
         L.drx_channel_generate.restype = ip
+        L.drx_ldpc_mix_new.argtypes = [ip, ctypes.POINTER(FecParams), ctypes.POINTER(cp)]
+        L.drx_ldpc_mix_new.restype = vp
+        L.drx_ldpc_mix_free.argtypes = [vp]
+        L.drx_ldpc_mix_plan.argtypes = [vp, ip, vp, vp, sz, vp, sz, vp, vp, ip]
+        L.drx_ldpc_mix_plan.restype = ip
+        L.drx_ldpc_mix_set_tiling.argtypes = [vp, ip]
+        L.drx_ldpc_mix_set_tiling.restype = ip
+        L.drx_ldpc_mix_tune.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+        L.drx_ldpc_mix_tune.restype = ip
+        L.drx_ldpc_mix_run.argtypes = [vp, vp]
+        L.drx_ldpc_mix_run.restype = ip
+        L.drx_ldpc_set_variant.argtypes = [vp, ip]
+        L.drx_ldpc_set_variant.restype = ip
         L.drx_ldpc_device_error.argtypes = [vp]
         L.drx_ldpc_device_error.restype = ip
         _lib = L
@@ -225,5 +239,91 @@ class Ldpc:
             raise RuntimeError("drx_channel_generate: " + last_error())
         return t_llr, t_info, t_h
 
+    def set_variant(self, variant):
+        """``drx_ldpc_set_variant``: VARIANT_AUTO, VARIANT_FRAME or
+        VARIANT_PAIR; returns the kernel per-frame batches now run."""
+        r = self._lib.drx_ldpc_set_variant(self.h, int(variant))
+        if r < 0:
+            raise ValueError("drx_ldpc_set_variant: " + last_error())
+        return r
+
     def device_error(self):
         return self._lib.drx_ldpc_device_error(self.h)
+
+
+TILING_ONE_LAUNCH, TILING_PER_CODE = 1, 2  # DRX_TILING_*
+
+
+class LdpcMix:
+    """A set of codes decoded together in mixed device batches
+    (``drx_ldpc_mix_*``): plan a batch once (captured as CUDA graphs), tune
+    the tiling on real frames, then replay it on new data in the same
+    buffers."""
+
+    def __init__(self, codes):
+        """codes: sequence of (short_frame, rate) or (FecParams, rate)."""
+        self._lib = lib()
+        params, rates = [], []
+        for a, rate in codes:
+            if isinstance(a, FecParams):
+                params.append(FecParams(a.short_frame, a.nldpc, a.kldpc, a.kbch, a.t))
+            else:
+                try:
+                    params.append(fec_lookup(a, rate))
+                except KeyError:  # codes without a BCH row (T2): nbch = K
+                    info = code_info(a, rate)
+                    params.append(FecParams(int(bool(a)), info.nldpc, info.K, info.K, 0))
+            rates.append(rate)
+        n = len(codes)
+        self.params = (FecParams * n)(*params)
+        self._rates = [r.encode() for r in rates]
+        self.rates = (ctypes.c_char_p * n)(*self._rates)
+        self.h = self._lib.drx_ldpc_mix_new(n, self.params, self.rates)
+        if not self.h:
+            raise RuntimeError("drx_ldpc_mix_new: " + last_error())
+        self.ncodes = n
+        self.nldpc = [p.nldpc for p in params]
+        self.nbytes = [(p.kldpc + 7) // 8 for p in params]
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.drx_ldpc_mix_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def plan(self, code, llr, out, iters, ok, max_iter):
+        """code: host int32 [n] code indexes; llr, out, iters, ok: torch CUDA
+        tensors [n, >= max nldpc] int8, [n, >= max bytes] uint8, [n] int32,
+        [n] uint8."""
+        code = np.ascontiguousarray(code, dtype=np.int32)
+        n = code.shape[0]
+        r = self._lib.drx_ldpc_mix_plan(self.h, n, code.ctypes.data, llr.data_ptr(), llr.stride(0),
+                                        out.data_ptr(), out.stride(0), iters.data_ptr(), ok.data_ptr(),
+                                        int(max_iter))
+        if r != 0:
+            raise RuntimeError("drx_ldpc_mix_plan: " + last_error())
+        self._keep = (llr, out, iters, ok)
+
+    def set_tiling(self, tiling):
+        if self._lib.drx_ldpc_mix_set_tiling(self.h, int(tiling)) < 0:
+            raise ValueError(last_error())
+
+    def tune(self, stream=None):
+        """Times both tilings on the planned batch; returns (choice,
+        ms_one_launch, ms_per_code)."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream()
+        a, b = ctypes.c_float(), ctypes.c_float()
+        r = self._lib.drx_ldpc_mix_tune(self.h, stream_handle(s), ctypes.byref(a), ctypes.byref(b))
+        if r < 0:
+            raise RuntimeError("drx_ldpc_mix_tune: " + last_error())
+        return r, a.value, b.value
+
+    def run(self, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream()
+        if self._lib.drx_ldpc_mix_run(self.h, stream_handle(s)) != 0:
+            raise RuntimeError("drx_ldpc_mix_run: " + last_error())

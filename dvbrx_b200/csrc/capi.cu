@@ -20,6 +20,7 @@
 #include "channel.h"
 #include "codes.h"
 #include "codes_gen.h"
+#include "handle.h"
 #include "ldpc_device.h"
 
 using namespace drxg;
@@ -42,35 +43,6 @@ constexpr int kLanes = 64;
 
 }  // namespace
 
-struct drx_ldpc {
-    int device = 0;
-    int sms = 0;
-    Code code;
-    drx_fec_params params{};
-    int nbytes = 0;
-    void* blob = nullptr; /* device: DevCode + tables */
-    DevCode* dcode = nullptr;
-    size_t smem = 0;
-    int ctas_per_sm = 0;
-    cudaStream_t stream = nullptr;
-    /* scratch */
-    void* msg = nullptr;
-    size_t msg_cap = 0;
-    unsigned* work = nullptr;
-    unsigned* sync = nullptr;
-    size_t sync_cap = 0;
-    int* err = nullptr;
-    /* staging of the host-pointer calls */
-    int8_t* h_llr = nullptr;
-    uint8_t* h_out = nullptr;
-    int32_t* h_it = nullptr;
-    uint8_t* h_ok = nullptr;
-    int8_t* d_llr = nullptr;
-    uint8_t* d_out = nullptr;
-    int32_t* d_it = nullptr;
-    uint8_t* d_ok = nullptr;
-    size_t stage_frames = 0;
-};
 
 namespace {
 
@@ -115,6 +87,29 @@ bool ensure_stage(drx_ldpc* d, size_t nframes)
     }
     d->stage_frames = nframes;
     return true;
+}
+
+bool ensure_scratch(drx_ldpc* d, size_t need)
+{
+    if (d->msg_cap >= need)
+        return true;
+    cudaStreamSynchronize(d->stream);
+    cudaFree(d->msg);
+    d->msg = nullptr;
+    d->msg_cap = 0;
+    if (!cuda_ok(cudaMalloc(&d->msg, need), "cudaMalloc(messages)"))
+        return false;
+    d->msg_cap = need;
+    return true;
+}
+
+/* The frame-pair kernel decodes per-frame batches of codes it supports,
+ * unless the handle is pinned to the one-frame kernel. */
+bool use_pair(const drx_ldpc* d)
+{
+    if (d->variant == DRX_VARIANT_FRAME)
+        return false;
+    return d->pair_ctas_per_sm > 0;
 }
 
 bool ensure_msg(drx_ldpc* d, int grid)
@@ -219,6 +214,20 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
     p.max_iter = max_iter;
     p.err = d->err;
     int grid;
+    if (stop == 0 && use_pair(d)) {
+        /* two frames per CTA */
+        grid = std::min((nframes + 1) / 2, d->pair_ctas_per_sm * d->sms);
+        p.group = 0;
+        p.work = d->work;
+        if (!cuda_ok(cudaMemsetAsync(d->work, 0, sizeof(unsigned), s), "cudaMemsetAsync"))
+            return -1;
+        const size_t slab = decode_pair_msg_bytes(d->code.R);
+        if (!ensure_scratch(d, slab * (size_t)grid))
+            return -1;
+        p.msg = d->msg;
+        p.msg_stride = slab;
+        return cuda_ok(launch_decode_pair(p, d->code.dclass, d->pair_smem, grid, s), "decoder launch") ? 0 : -1;
+    }
     if (stop == 0) {
         grid = std::min(nframes, capacity);
         p.group = 0;
@@ -312,6 +321,11 @@ drx_ldpc* drx_ldpc_new(const drx_fec_params* p, const char* rate)
         return nullptr;
     }
     d->ctas_per_sm = decode_ctas_per_sm(d->code.dclass, d->smem);
+    if (pair_supported(d->code.dclass)) {
+        d->pair_smem = decode_pair_smem_bytes(d->code.N, (int)d->code.ent.size() / 2,
+                                              (int)d->code.steps.size(), d->code.q);
+        d->pair_ctas_per_sm = decode_pair_ctas_per_sm(d->code.dclass, d->pair_smem);
+    }
     if (d->ctas_per_sm <= 0) {
         set_err("decoder kernel does not fit on this device");
         drx_ldpc_free(d);
@@ -351,6 +365,20 @@ int drx_ldpc_get_info(const drx_ldpc* d, drx_ldpc_info* info)
     info->deg_max = d->code.deg_max;
     info->levelled = d->code.levelled ? 1 : 0;
     return 0;
+}
+
+int drx_ldpc_set_variant(drx_ldpc* d, int variant)
+{
+    if (!d || (variant != DRX_VARIANT_AUTO && variant != DRX_VARIANT_FRAME && variant != DRX_VARIANT_PAIR)) {
+        set_err("unknown variant");
+        return -1;
+    }
+    if (variant == DRX_VARIANT_PAIR && d->pair_ctas_per_sm <= 0) {
+        set_err("the frame-pair kernel does not run this code");
+        return -1;
+    }
+    d->variant = variant;
+    return use_pair(d) ? DRX_VARIANT_PAIR : DRX_VARIANT_FRAME;
 }
 
 int drx_ldpc_code_info(int short_frame, const char* rate, drx_ldpc_info* info)
@@ -554,5 +582,12 @@ const DevCode* handle_code(const drx_ldpc* d, int* R, int* dclass, int* N, int* 
 }
 
 void handle_set_error(const char* msg) { set_err(msg); }
+
+}  // namespace drxg
+
+namespace drxg {
+
+void set_error(const std::string& s) { set_err(s); }
+bool cuda_check(cudaError_t e, const char* what) { return cuda_ok(e, what); }
 
 }  // namespace drxg

@@ -1,0 +1,55 @@
+/*
+ * The decoder handle (drx_ldpc) and the host helpers shared by the C-ABI
+ * files (capi.cu, mix.cu).
+ */
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/dvbrx_b200.h"
+#include "codes.h"
+#include "ldpc_device.h"
+
+using drxg::Code;
+using drxg::DevCode;
+
+struct drx_ldpc {
+    int device = 0;
+    int sms = 0;
+    Code code;
+    drx_fec_params params{};
+    int nbytes = 0;
+    void* blob = nullptr; /* device: DevCode + tables */
+    DevCode* dcode = nullptr;
+    size_t smem = 0;
+    int ctas_per_sm = 0;
+    size_t pair_smem = 0;
+    int pair_ctas_per_sm = 0; /* 0: the frame-pair kernel does not run this code */
+    int variant = DRX_VARIANT_AUTO;
+    cudaStream_t stream = nullptr;
+    /* scratch */
+    void* msg = nullptr;
+    size_t msg_cap = 0;
+    unsigned* work = nullptr;
+    unsigned* sync = nullptr;
+    size_t sync_cap = 0;
+    int* err = nullptr;
+    /* staging of the host-pointer calls */
+    int8_t* h_llr = nullptr;
+    uint8_t* h_out = nullptr;
+    int32_t* h_it = nullptr;
+    uint8_t* h_ok = nullptr;
+    int8_t* d_llr = nullptr;
+    uint8_t* d_out = nullptr;
+    int32_t* d_it = nullptr;
+    uint8_t* d_ok = nullptr;
+    size_t stage_frames = 0;
+};
+
+namespace drxg {
+
+void set_error(const std::string& s);
+bool cuda_check(cudaError_t e, const char* what);
+
+}  // namespace drxg

@@ -353,8 +353,9 @@ __device__ void decode_frame(const DevCode& c, const Frame& fr, const DecodePara
                              typename MsgWord<DMAX>::T* msg, volatile int* sflag, unsigned* sync)
 {
     const bool real = f < p.nframes;
+    const int row = real && p.rows ? p.rows[f] : f;
     if (real)
-        load_frame(c, fr, p.llr + (size_t)f * p.llr_stride);
+        load_frame(c, fr, p.llr + (size_t)row * p.llr_stride);
     __syncthreads();
     int it = 0;
     bool ok = true;
@@ -379,12 +380,12 @@ __device__ void decode_frame(const DevCode& c, const Frame& fr, const DecodePara
         it++;
     }
     if (real) {
-        store_bits(c, fr, p.out + (size_t)f * p.out_stride);
+        store_bits(c, fr, p.out + (size_t)row * p.out_stride);
         if (threadIdx.x == 0) {
             if (p.iters)
-                p.iters[f] = it;
+                p.iters[row] = it;
             if (p.ok)
-                p.ok[f] = ok ? 1 : 0;
+                p.ok[row] = ok ? 1 : 0;
         }
     }
     __syncthreads();
@@ -424,6 +425,91 @@ __global__ void __launch_bounds__(kThreads, MINB) k_decode(DecodeParams p)
             decode_frame<DMAX>(c, fr, p, g * G + member, msg, &s_flag, sync);
         }
     }
+}
+
+/* Mixed batch, one launch: frames of several codes in `order` (longest
+ * work first), one frame per CTA; the code tables are restaged when the
+ * next frame's code differs from the one in shared memory. */
+template <int DMAX, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_decode_mix(MixParams mp)
+{
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_k;
+    __shared__ int s_flag;
+    typedef typename MsgWord<DMAX>::T W;
+    W* msg = (W*)((char*)mp.msg + (size_t)blockIdx.x * mp.msg_stride);
+    DecodeParams p{};
+    p.llr = mp.llr;
+    p.llr_stride = mp.llr_stride;
+    p.out = mp.out;
+    p.out_stride = mp.out_stride;
+    p.iters = mp.iters;
+    p.ok = mp.ok;
+    p.nframes = mp.nframes;
+    p.max_iter = mp.max_iter;
+    p.rows = mp.order;
+    if (threadIdx.x == 0)
+        s_flag = 0;
+    int staged = -1;
+    DevCode c{};
+    Frame fr{};
+    for (;;) {
+        if (threadIdx.x == 0)
+            s_k = (int)atomicAdd(mp.work, 1u);
+        __syncthreads();
+        const int k = s_k;
+        __syncthreads();
+        if (k >= mp.nframes)
+            break;
+        const int ci = mp.frame_code[mp.order[k]];
+        if (ci != staged) {
+            c = *mp.codes[ci];
+            fr = stage_code(c, smem);
+            staged = ci;
+            __syncthreads();
+        }
+        decode_frame<DMAX>(c, fr, p, k, msg, &s_flag, nullptr);
+    }
+}
+
+static const void* mix_kernel_for(int dclass)
+{
+    switch (dclass) {
+    case 0:
+        return (const void*)k_decode_mix<7, 4>;
+    case 1:
+        return (const void*)k_decode_mix<11, 3>;
+    case 2:
+        return (const void*)k_decode_mix<14, 3>;
+    case 3:
+        return (const void*)k_decode_mix<18, 2>;
+    case 4:
+        return (const void*)k_decode_mix<22, 2>;
+    default:
+        return (const void*)k_decode_mix<32, 1>;
+    }
+}
+
+int decode_mix_ctas_per_sm(int dclass, size_t smem)
+{
+    const void* k = mix_kernel_for(dclass);
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kThreads, smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+cudaError_t launch_decode_mix(const MixParams& p, int dclass, size_t smem, int grid, cudaStream_t stream)
+{
+    const void* k = mix_kernel_for(dclass);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    MixParams pc = p;
+    void* args[] = { &pc };
+    return cudaLaunchKernel(k, dim3(grid), dim3(kThreads), args, smem, stream);
 }
 
 size_t decode_smem_bytes(int N, int nent, int nsteps, int q)

@@ -41,7 +41,33 @@ struct DecodeParams {
     void* msg;             /* message scratch: grid * msg_stride bytes */
     size_t msg_stride;
     int* err;              /* device error word (0 = fine) */
+    const int32_t* rows;   /* per-frame mode, optional: work item k is row rows[k] of
+                              llr / out / iters / ok (null: row k) */
 };
+
+/* A batch of frames of several codes (one launch over all of them). */
+struct MixParams {
+    const DevCode* const* codes; /* device array: code of each code index */
+    const int32_t* frame_code;   /* code index of every row */
+    const int32_t* order;        /* rows in processing order (nframes) */
+    const int8_t* llr;
+    size_t llr_stride;
+    uint8_t* out;
+    size_t out_stride;
+    int32_t* iters;
+    uint8_t* ok;
+    int nframes;
+    int max_iter;
+    unsigned* work;
+    void* msg;
+    size_t msg_stride;
+};
+
+/* One persistent launch over a mixed batch: one frame per CTA, the CTA
+ * restages the code tables in shared memory when the next frame's code
+ * differs.  `dclass` is the largest degree class of the mix. */
+cudaError_t launch_decode_mix(const MixParams& p, int dclass, size_t smem, int grid, cudaStream_t stream);
+int decode_mix_ctas_per_sm(int dclass, size_t smem);
 
 /* Largest dynamic shared memory of the plain kernel for a code. */
 size_t decode_smem_bytes(int N, int nent, int nsteps, int q);
@@ -54,5 +80,17 @@ int decode_ctas_per_sm(int dclass, size_t smem);
  * launch (co-resident CTAs are required by the group barrier). */
 cudaError_t launch_decode(const DecodeParams& p, int dclass, size_t smem, int grid,
                           cudaStream_t stream);
+
+}  // namespace drxg
+
+namespace drxg {
+
+/* Frame-pair variant (ldpc_pair.cu): two frames per CTA in 16x2 SIMD, codes
+ * up to check degree 16; per-frame stopping only. */
+bool pair_supported(int dclass);
+size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q);
+size_t decode_pair_msg_bytes(int R);
+int decode_pair_ctas_per_sm(int dclass, size_t smem);
+cudaError_t launch_decode_pair(const DecodeParams& p, int dclass, size_t smem, int grid, cudaStream_t stream);
 
 }  // namespace drxg

@@ -1,0 +1,496 @@
+/*
+ * Plain decoder, frame-pair variant: the same arithmetic as ldpc_decode.cu
+ * (bit-exact to libdvbrx/src/ldpc.c), two frames per CTA.
+ *
+ * SIMD within a register: every value of the decoder fits 16 bits, so each
+ * 32-bit register carries the same quantity for two frames, lane A in the
+ * low half and lane B in the high half, and every step of the check node is
+ * a native 16x2 instruction on sm_100a (video min/max __vmins2/__vmaxs2,
+ * DPX __viaddmax_s16x2 for the saturating add, lane-wise __vsub2/__vneg2,
+ * PRMT for sign masks and byte packing, an FP16 compare for the message
+ * index).  One instruction stream decodes two frames.
+ *
+ * Shared memory holds both frames' posteriors interleaved: the 16-bit word
+ * v holds the int8 posterior of variable v for lane A (low byte) and lane B
+ * (high byte): K information bits, then R parity bits in layer order.
+ *
+ * A check node is spread over L lanes of a warp (its links c = r, r + L, ...
+ * go to lane r): L = 2 on the full 360-check steps, L = 4 or 8 on the small
+ * steps of levelled layers, so that the serial part of a step (a check
+ * node's chain over its links) is short where few checks can run.  The
+ * lanes combine their two smallest magnitudes and sign parities with
+ * shuffles, then each writes its own links' outputs; the group's first lane
+ * stores the check's compressed messages for both frames in one 8-byte
+ * record: per lane min0 (6 bits) | min1 << 6 | index << 12, then the sign
+ * bits of lane A in the low half and of lane B in the high half.
+ *
+ * Frames stream through the two lanes independently: when a lane's frame
+ * passes the syndrome check or reaches max_iter, its results are written
+ * and the lane takes the next frame of the batch (its first iteration reads
+ * zero messages), so a converged frame never waits for its neighbour.
+ * Codes up to check degree 16 (degree classes 0-2) run here.
+ */
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "codes.h"
+#include "ldpc_device.h"
+
+namespace drxg {
+
+constexpr int kPT = 768; /* threads of a pair CTA */
+constexpr int kQCp = 360;
+
+/* PRMT in its default mode: a selector nibble with bit 3 set replicates the
+ * sign bit of the selected byte.  (__byte_perm keeps only the low 3 bits of
+ * each nibble, so the sign-replicating forms need the instruction itself.) */
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel)
+{
+    uint32_t d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+    return d;
+}
+/* two int8 (low 16 bits) -> int16x2, sign-extended */
+__device__ __forceinline__ uint32_t sx2(uint32_t b) { return prmt(b, 0, 0x9180); }
+/* int16x2 in [-128, 127] -> two bytes (low 16 bits) */
+__device__ __forceinline__ uint32_t pk2(uint32_t v) { return prmt(v, 0, 0x0020); }
+/* 0xFFFF in each lane whose bit 15 is set */
+__device__ __forceinline__ uint32_t lmask(uint32_t v) { return prmt(v, 0, 0xBB99); }
+__device__ __forceinline__ uint32_t sel(uint32_t m, uint32_t a, uint32_t b) { return (m & a) | (~m & b); }
+/* saturating int8 add in int16 lanes */
+__device__ __forceinline__ uint32_t sadd(uint32_t a, uint32_t b)
+{
+    return __vmins2(__viaddmax_s16x2(a, b, 0xFF80FF80u), 0x007F007Fu);
+}
+/* lane-wise negation and |x|: __vsub2 issues on the FMA pipe, leaving the
+ * (half-rate) ALU pipe to the min/max, select and permute work */
+__device__ __forceinline__ uint32_t neg2(uint32_t x) { return __vsub2(0u, x); }
+__device__ __forceinline__ uint32_t abs2(uint32_t x) { return __vmaxs2(x, neg2(x)); }
+__device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
+{
+    return __heq2_mask(*(const __half2*)&a, *(const __half2*)&b);
+}
+
+/*
+ * Check node (i, j) for both lanes, spread over L threads (lane r of the
+ * group).  Slots: 0 = parity bit, 1 = previous parity bit (absent for
+ * (0, 0)), 2.. = information bits.
+ */
+template <int CNT, int L>
+__device__ __forceinline__ void check_pair(uint16_t* __restrict__ post, const int2* __restrict__ ent,
+                                           int K, int q, int i, int j, int r, uint2 rec, uint32_t fresh,
+                                           unsigned gmask, uint2* __restrict__ dst)
+{
+    constexpr int D = CNT + 2;
+    constexpr int S = (D + L - 1) / L;
+    const bool has_pp = (i | j) != 0;
+    const int pc = K + kQCp * i + j;
+    const int pp = i ? pc - kQCp : K + kQCp * (q - 1) + j - 1;
+
+    /* this lane's slots: c = r + k L */
+    int addr[S];
+    bool live[S];
+#pragma unroll
+    for (int k = 0; k < S; k++) {
+        const int c = r + k * L;
+        live[k] = c < D && (c != 1 || has_pp);
+        int a = 0;
+        if (k == 0 && L > 2) {
+            a = c == 0 ? pc : c == 1 ? pp : 0;
+        } else if (k == 0) {
+            a = r == 0 ? pc : pp; /* L <= 2: slot r is a parity slot */
+        }
+        const bool info = (k > 0) || (c >= 2);
+        if (info && c < D) {
+            const int2 e = ent[c - 2];
+            a = e.x + j + (j < e.y ? kQCp : 0);
+        }
+        addr[k] = a;
+    }
+    /* messages of the check: zero for a lane in its first iteration */
+    const uint32_t w0 = rec.x & ~fresh, sgn = rec.y & ~fresh;
+    const uint32_t m0 = w0 & 0x003F003Fu, m1 = (w0 >> 6) & 0x003F003Fu;
+    const uint32_t idxh = ((w0 >> 12) & 0x000F000Fu) | 0x64006400u; /* FP16 1024 + index */
+    /* minus the message: +m if it is negative, else -min(m, 31) */
+    const uint32_t n0 = m0, n1 = m1;
+    const uint32_t p0 = neg2(__vmins2(m0, 0x001F001Fu)), p1 = neg2(__vmins2(m1, 0x001F001Fu));
+
+    uint32_t x[S];
+    uint32_t min0 = 0x00FF00FFu, min1 = 0x00FF00FFu, sg = 0;
+#pragma unroll
+    for (int k = 0; k < S; k++) {
+        const int c = r + k * L;
+        uint32_t v = 0x00FF00FFu; /* absent link: 255 in both lanes */
+        if (live[k]) {
+            v = sx2(post[addr[k]]);
+            const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)c * 0x00010001u);
+            const uint32_t sm = lmask(sgn << (15 - c));
+            const uint32_t nm = sel(sm, sel(im, n1, n0), sel(im, p1, p0));
+            v = sadd(v, nm);
+        }
+        x[k] = v;
+        const uint32_t a = abs2(v);
+        min1 = __vmins2(min1, __vmaxs2(min0, a));
+        min0 = __vmins2(min0, a);
+        sg ^= v;
+    }
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1) {
+        const uint32_t b0 = __shfl_xor_sync(gmask, min0, o);
+        const uint32_t b1 = __shfl_xor_sync(gmask, min1, o);
+        const uint32_t bs = __shfl_xor_sync(gmask, sg, o);
+        min1 = __vmins2(__vmaxs2(min0, b0), __vmins2(min1, b1));
+        min0 = __vmins2(min0, b0);
+        sg ^= bs;
+    }
+    /* offset 1 and the cap at 127, once per node */
+    const uint32_t mn0 = __viaddmax_s16x2(__vmins2(min0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+    const uint32_t mn1 = __viaddmax_s16x2(__vmins2(min1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+    const uint32_t min0p1 = __vadd2(min0, 0x00010001u);
+    uint32_t nidx = 0, nsg = 0;
+#pragma unroll
+    for (int k = 0; k < S; k++) {
+        const int c = r + k * L;
+        const uint32_t v = x[k];
+        const uint32_t eq = lmask(__vsub2(abs2(v), min0p1)); /* |x| == min0 */
+        const uint32_t mag = sel(eq, mn1, mn0);
+        const uint32_t sm = lmask(sg ^ v);
+        const uint32_t o = __vsub2(mag ^ sm, sm);
+        if (live[k])
+            post[addr[k]] = (uint16_t)pk2(sadd(v, o));
+        if (c < D) {
+            nidx = sel(eq, (uint32_t)c * 0x00010001u, nidx);
+            nsg |= sm & (0x00010001u << c);
+        }
+    }
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1) {
+        nidx = __vmaxs2(nidx, __shfl_xor_sync(gmask, nidx, o));
+        nsg |= __shfl_xor_sync(gmask, nsg, o);
+    }
+    if (r == 0) {
+        const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
+        __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
+    }
+}
+
+template <int DMAX>
+struct PairLanes {
+    static constexpr int part = DMAX <= 8 ? 4 : 8; /* lanes per check on small steps */
+};
+
+template <int DMAX>
+__device__ __forceinline__ void check_pair_dispatch(int cnt, int L, uint16_t* post, const int2* ent, int K,
+                                                    int q, int i, int j, int r, uint2 rec, uint32_t fresh,
+                                                    unsigned gmask, uint2* dst)
+{
+    constexpr int LP = PairLanes<DMAX>::part;
+#define DRXG_PCASE(n)                                                                                \
+    case n:                                                                                          \
+        if (n + 2 <= DMAX) {                                                                         \
+            if (L == 2)                                                                              \
+                check_pair<(n + 2 <= DMAX ? n : 1), 2>(post, ent, K, q, i, j, r, rec, fresh, gmask, dst); \
+            else                                                                                     \
+                check_pair<(n + 2 <= DMAX ? n : 1), LP>(post, ent, K, q, i, j, r, rec, fresh, gmask, dst); \
+        }                                                                                            \
+        break;
+    switch (cnt) {
+        DRXG_PCASE(1) DRXG_PCASE(2) DRXG_PCASE(3) DRXG_PCASE(4) DRXG_PCASE(5) DRXG_PCASE(6)
+        DRXG_PCASE(7) DRXG_PCASE(8) DRXG_PCASE(9) DRXG_PCASE(10) DRXG_PCASE(11) DRXG_PCASE(12)
+        DRXG_PCASE(13) DRXG_PCASE(14)
+    default:
+        break;
+    }
+#undef DRXG_PCASE
+}
+
+struct PairFrame {
+    uint16_t* post;
+    const int2* ent;
+    const uint16_t* eoff;
+    const uint32_t* steps;
+};
+
+__device__ __forceinline__ size_t a16p(size_t v) { return (v + 15) & ~(size_t)15; }
+
+__device__ PairFrame stage_pair(const DevCode& c, char* smem)
+{
+    PairFrame f;
+    f.post = (uint16_t*)smem;
+    size_t off = a16p(2 * (size_t)c.N);
+    int2* ent = (int2*)(smem + off);
+    off += a16p(sizeof(int2) * c.nent);
+    uint16_t* eoff = (uint16_t*)(smem + off);
+    off += a16p(sizeof(uint16_t) * (c.q + 1));
+    uint32_t* steps = (uint32_t*)(smem + off);
+    for (int k = threadIdx.x; k < c.nent; k += blockDim.x)
+        ent[k] = c.ent[k];
+    for (int k = threadIdx.x; k <= c.q; k += blockDim.x)
+        eoff[k] = c.eoff[k];
+    for (int k = threadIdx.x; k < c.nsteps; k += blockDim.x)
+        steps[k] = c.steps[k];
+    f.ent = ent;
+    f.eoff = eoff;
+    f.steps = steps;
+    return f;
+}
+
+/* Frame f's LLRs into byte `h` of every posterior word (f < 0: the all-zero
+ * codeword at full confidence, which passes every check). */
+__device__ void load_lane(const DevCode& c, const PairFrame& fr, const int8_t* __restrict__ src, int h)
+{
+    uint8_t* b = (uint8_t*)fr.post + h;
+    const int t = threadIdx.x;
+    if (!src) {
+        for (int v = t; v < c.N; v += blockDim.x)
+            b[2 * v] = 127;
+        return;
+    }
+    if (((uintptr_t)src & 7) == 0) {
+        const uint2* s8 = (const uint2*)src;
+        for (int u = t; u < c.K / 8; u += blockDim.x) {
+            const uint2 w = __ldcs(s8 + u);
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+                b[2 * (8 * u + r)] = (uint8_t)((r < 4 ? w.x : w.y) >> (8 * (r & 3)));
+        }
+        const uint32_t qm = 0xFFFFFFFFu / (uint32_t)c.q + 1u;
+        for (int u = t; u < c.R / 8; u += blockDim.x) {
+            const uint2 w = __ldcs(s8 + c.K / 8 + u);
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const uint32_t k = 8u * u + r;
+                const uint32_t jj = __umulhi(k, qm), ii = k - jj * c.q;
+                b[2 * (c.K + kQCp * ii + jj)] = (uint8_t)((r < 4 ? w.x : w.y) >> (8 * (r & 3)));
+            }
+        }
+    } else {
+        for (int v = t; v < c.K; v += blockDim.x)
+            b[2 * v] = (uint8_t)src[v];
+        for (int k = t; k < c.R; k += blockDim.x)
+            b[2 * (c.K + kQCp * (k % c.q) + k / c.q)] = (uint8_t)src[c.K + k];
+    }
+}
+
+/* Syndrome of both lanes: bit h of the result set if lane h fails.  Thread
+ * t checks column t % 360 of every other layer; the scan stops once both
+ * lanes have failed. */
+__device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int* sflag)
+{
+    const int t = threadIdx.x;
+    const int nh = blockDim.x / kQCp; /* threads per column */
+    int fail = 0;
+    if (t < nh * kQCp) {
+        const int j = t % kQCp, h0 = t / kQCp;
+        const uint16_t* post = fr.post;
+        for (int i = h0; i < c.q; i += nh) {
+            if (*sflag == 3)
+                break;
+            const uint32_t pc = sx2(post[c.K + kQCp * i + j]);
+            const uint32_t pp = i ? sx2(post[c.K + kQCp * (i - 1) + j])
+                                  : (j ? sx2(post[c.K + kQCp * (c.q - 1) + j - 1]) : 0x00010001u);
+            uint32_t par = pc ^ pp;
+            uint32_t z = (__vsub2(pc, 0x00010001u) & ~pc) | (__vsub2(pp, 0x00010001u) & ~pp);
+            const int e1 = fr.eoff[i + 1];
+            for (int e = fr.eoff[i]; e < e1; e++) {
+                const int2 en = fr.ent[e];
+                const uint32_t v = sx2(post[en.x + j + (j < en.y ? kQCp : 0)]);
+                par ^= v;
+                z |= __vsub2(v, 0x00010001u) & ~v;
+            }
+            const uint32_t bad = (par | z);
+            const int f = ((bad >> 15) & 1) | ((bad >> 30) & 2);
+            if (f & ~fail) {
+                fail |= f;
+                atomicOr((int*)sflag, f);
+            }
+        }
+    }
+    __syncthreads();
+    const int r = *sflag;
+    __syncthreads();
+    return r;
+}
+
+template <int DMAX>
+__device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __restrict__ msg, uint32_t fresh)
+{
+    constexpr int LP = PairLanes<DMAX>::part;
+    const int t = threadIdx.x;
+    auto lanes = [&](int n) { return n * LP <= (int)blockDim.x ? LP : 2; };
+    uint2 rn = make_uint2(0, 0);
+    int jn = 0;
+    auto fetch = [&](int s, uint2& rec, int& jj) {
+        const uint32_t st = fr.steps[s];
+        const int i = st & 0xFF, start = (st >> 8) & 0x1FF, n = (st >> 17) & 0x1FF;
+        const int L = lanes(n);
+        const int g = t / L;
+        if (g < n) {
+            const int pos = start + g;
+            jj = (st >> 26) ? (int)__ldg(c.perm + kQCp * i + pos) : pos;
+            rec = __ldcg(msg + kQCp * i + pos);
+        }
+    };
+    fetch(0, rn, jn);
+    for (int s = 0; s < c.nsteps; s++) {
+        const uint2 rec = rn;
+        const int j = jn;
+        const uint32_t st = fr.steps[s];
+        const int i = st & 0xFF, start = (st >> 8) & 0x1FF, n = (st >> 17) & 0x1FF;
+        if (s + 1 < c.nsteps)
+            fetch(s + 1, rn, jn);
+        const int L = lanes(n);
+        const int g = t / L, r = t % L;
+        const unsigned gmask = __ballot_sync(0xFFFFFFFFu, g < n);
+        if (g < n) {
+            const int e0 = fr.eoff[i];
+            check_pair_dispatch<DMAX>(fr.eoff[i + 1] - e0, L, fr.post, fr.ent + e0, c.K, c.q, i, j, r, rec,
+                                      fresh, gmask, msg + kQCp * i + start + g);
+        }
+        __syncthreads();
+    }
+}
+
+__device__ void store_lane(const DevCode& c, const PairFrame& fr, int h, uint8_t* __restrict__ dst)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int8_t* b = (const int8_t*)fr.post + h;
+    const int nchunks = (c.kldpc + 31) / 32;
+    for (int ch = warp; ch < nchunks; ch += nw) {
+        const int v = ch * 32 + lane;
+        const int x = v < c.kldpc ? b[2 * v] : 0;
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, x < 0);
+        const unsigned rr = __byte_perm(__brev(m), 0, 0x0123);
+        if (lane < 4 && 4 * ch + lane < c.nbytes)
+            dst[4 * ch + lane] = (uint8_t)(rr >> (8 * lane));
+    }
+}
+
+template <int DMAX, int MINB>
+__global__ void __launch_bounds__(kPT, MINB) k_decode_pair(DecodeParams p)
+{
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_frame[2], s_iter[2], s_flag, s_reload;
+    const DevCode c = *p.code;
+    const PairFrame fr = stage_pair(c, smem);
+    uint2* msg = (uint2*)((char*)p.msg + (size_t)blockIdx.x * p.msg_stride);
+    const int t = threadIdx.x;
+    if (t == 0) {
+        s_frame[0] = s_frame[1] = -1;
+        s_flag = 0;
+        s_reload = 3;
+    }
+    __syncthreads();
+    uint32_t fresh = 0;
+    for (;;) {
+        /* lanes that need a frame take the next one of the batch */
+        const int reload = s_reload;
+        if (reload) {
+            if (t == 0) {
+                for (int h = 0; h < 2; h++)
+                    if (reload & (1 << h)) {
+                        const int f = (int)atomicAdd(p.work, 1u);
+                        s_frame[h] = f < p.nframes ? f : -1;
+                        s_iter[h] = 0;
+                    }
+            }
+            __syncthreads();
+            for (int h = 0; h < 2; h++)
+                if (reload & (1 << h)) {
+                    const int f = s_frame[h];
+                    const int row = f < 0 ? 0 : p.rows ? p.rows[f] : f;
+                    load_lane(c, fr, f >= 0 ? p.llr + (size_t)row * p.llr_stride : nullptr, h);
+                    fresh |= 0xFFFFu << (16 * h);
+                }
+            if (t == 0)
+                s_reload = 0;
+            __syncthreads();
+        }
+        if (s_frame[0] < 0 && s_frame[1] < 0)
+            break;
+        const int fail = syndrome_pair(c, fr, &s_flag);
+        /* lanes whose frame is done: results out, refill */
+        int done = 0;
+        for (int h = 0; h < 2; h++) {
+            const int f = s_frame[h];
+            if (f >= 0 && (!((fail >> h) & 1) || s_iter[h] >= p.max_iter)) {
+                const int row = p.rows ? p.rows[f] : f;
+                store_lane(c, fr, h, p.out + (size_t)row * p.out_stride);
+                if (t == 0) {
+                    if (p.iters)
+                        p.iters[row] = s_iter[h];
+                    if (p.ok)
+                        p.ok[row] = (fail >> h) & 1 ? 0 : 1;
+                }
+                done |= 1 << h;
+            }
+        }
+        __syncthreads();
+        if (t == 0) {
+            s_flag = 0;
+            s_reload = done;
+        }
+        __syncthreads();
+        if (done)
+            continue; /* reload, then check the new frames first */
+        iterate_pair<DMAX>(c, fr, msg, fresh);
+        fresh = 0;
+        if (t == 0) {
+            s_iter[0]++;
+            s_iter[1]++;
+        }
+        __syncthreads();
+    }
+}
+
+size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q)
+{
+    auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+    return a16(2 * (size_t)N) + a16(sizeof(int2) * nent) + a16(sizeof(uint16_t) * (q + 1)) +
+           a16(sizeof(uint32_t) * nsteps);
+}
+
+size_t decode_pair_msg_bytes(int R) { return (size_t)R * sizeof(uint2); }
+
+bool pair_supported(int dclass) { return dclass >= 0 && dclass <= 2; }
+
+static const void* pair_kernel(int dclass)
+{
+    switch (dclass) {
+    case 0:
+        return (const void*)k_decode_pair<7, 1>;
+    case 1:
+        return (const void*)k_decode_pair<11, 1>;
+    default:
+        return (const void*)k_decode_pair<14, 1>;
+    }
+}
+
+int decode_pair_ctas_per_sm(int dclass, size_t smem)
+{
+    if (!pair_supported(dclass))
+        return 0;
+    const void* k = pair_kernel(dclass);
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kPT, smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+cudaError_t launch_decode_pair(const DecodeParams& p, int dclass, size_t smem, int grid, cudaStream_t stream)
+{
+    if (!pair_supported(dclass))
+        return cudaErrorInvalidValue;
+    const void* k = pair_kernel(dclass);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    DecodeParams pc = p;
+    void* args[] = { &pc };
+    return cudaLaunchKernel(k, dim3(grid), dim3(kPT), args, smem, stream);
+}
+
+}  // namespace drxg

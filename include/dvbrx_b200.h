@@ -136,6 +136,51 @@ int drx_channel_generate(drx_ldpc* d, const char* constellation, const char* con
                          void* llr_f16, size_t llr_f16_stride, uint8_t* info, size_t info_stride,
                          void* stream);
 
+/* Kernel of the per-frame batch calls: DRX_VARIANT_AUTO (the default) runs
+ * the frame-pair kernel (two frames per CTA, 16x2 SIMD) for codes up to
+ * check degree 14 and the one-frame kernel otherwise; DRX_VARIANT_FRAME
+ * pins the one-frame kernel.  Both give identical results.  Returns the
+ * variant per-frame batches will now run (DRX_VARIANT_FRAME or
+ * DRX_VARIANT_PAIR), or -1. */
+#define DRX_VARIANT_AUTO 0
+#define DRX_VARIANT_FRAME 1
+#define DRX_VARIANT_PAIR 2
+int drx_ldpc_set_variant(drx_ldpc* d, int variant);
+
+/* ---- mixed batches: several codes (MODCODs, normal and short) at once ---- */
+
+typedef struct drx_ldpc_mix drx_ldpc_mix;
+
+/* A set of ncodes codes (params[c], rates[c]); code index c refers to the
+ * c-th.  NULL on failure (drx_ldpc_last_error()). */
+drx_ldpc_mix* drx_ldpc_mix_new(int ncodes, const drx_fec_params* params, const char* const* rates);
+void drx_ldpc_mix_free(drx_ldpc_mix* m);
+
+/* Plan a device batch of nframes rows: row f holds a frame of code code[f]
+ * (host array) at llr + f * llr_stride, its bits go to out + f * out_stride,
+ * its iterations and flag to iters[f] and ok[f] (device; may be NULL).
+ * Strides must fit the largest code of the set.  Per-frame stopping.  The
+ * plan is captured as CUDA graphs, one per tiling, replayed by
+ * drx_ldpc_mix_run on whatever the buffers hold at that time. */
+int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* llr, size_t llr_stride,
+                      uint8_t* out, size_t out_stride, int32_t* iters, uint8_t* ok, int max_iter);
+
+/* Tilings of a mixed batch (identical results): one persistent launch over
+ * all frames, one frame per CTA; or one persistent launch per code with the
+ * code's own kernel (two frames per CTA where the frame-pair kernel
+ * applies) on concurrent graph branches. */
+#define DRX_TILING_ONE_LAUNCH 1
+#define DRX_TILING_PER_CODE 2
+int drx_ldpc_mix_set_tiling(drx_ldpc_mix* m, int tiling);
+
+/* Autotuner: decodes the planned batch with each tiling (twice, after a
+ * warm-up), keeps the faster and returns it; the times in ms if non-NULL.
+ * Synchronous. */
+int drx_ldpc_mix_tune(drx_ldpc_mix* m, void* stream, float* ms_one_launch, float* ms_per_code);
+
+/* Launch the plan's graph (the tuned or set tiling) on `stream`. */
+int drx_ldpc_mix_run(drx_ldpc_mix* m, void* stream);
+
 /* Device error word of the handle: 0, or the code of a device-side fault
  * report (2: a group barrier timed out).  Cleared by the call. */
 int drx_ldpc_device_error(drx_ldpc* d);

@@ -172,3 +172,36 @@ def test_device_batch_strided():
     assert (out[:, : d.nbytes].cpu().numpy() == ref[0]).all()
     assert (it.cpu().numpy() == ref[1]).all() and (ok.cpu().numpy() == ref[2]).all()
     assert (out[:, d.nbytes:].cpu().numpy() == 0).all()
+
+
+@pytest.mark.parametrize("short,rate,const,es,n,max_iter", [
+    (1, "1_2", "QPSK", 1.5, 41, 50),
+    (0, "3_5", "8PSK", 5.6, 17, 30),
+    (0, "2_3", "8PSK", 6.4, 9, 20),
+    (1, "3_5", "QPSK", 2.8, 33, 25),
+    (0, "13_45", "QPSK", -0.8, 5, 30),
+    (0, "1_4", "QPSK", -1.0, 5, 30),
+    (1, "8_15", "QPSK", 2.4, 31, 30),
+    (0, "3_5", "8PSK", 6.0, 3, 0),
+])
+def test_kernel_variants_agree(short, rate, const, es, n, max_iter):
+    """The one-frame kernel and the frame-pair kernel (odd frame counts leave
+    a lane empty at the end) both reproduce the reference."""
+    llr = awgn_frames(short, rate, n, es, seed=zlib.crc32(rate.encode()) + 17 * n, constellation=const)
+    rb, ri, ro = check_frames(checker(short, rate), llr, max_iter)
+    p = D.fec_lookup(short, rate)
+    d = D.Ldpc(p, rate)
+    for v in (D.VARIANT_FRAME, D.VARIANT_PAIR):
+        assert d.set_variant(v) == v
+        bits, it, ok = d.decode_host(llr, max_iter)
+        assert (bits == rb).all() and (it == ri).all() and (ok == ro).all(), "variant %d" % v
+    d.close()
+
+
+def test_variant_auto_choice():
+    d = handle(0, "3_5")
+    assert d.set_variant(D.VARIANT_AUTO) == D.VARIANT_PAIR
+    hi = handle(0, "9_10")  # check degree 30: one-frame kernel only
+    assert hi.set_variant(D.VARIANT_AUTO) == D.VARIANT_FRAME
+    with pytest.raises(ValueError):
+        hi.set_variant(D.VARIANT_PAIR)

@@ -1,0 +1,94 @@
+"""Mixed batches (several MODCODs, normal and short frames, one batch) through
+drx_ldpc_mix_*: every tiling, and the autotuner's choice, give the results
+of one-code decodes, which are themselves bit-exact to the reference."""
+import numpy as np
+import pytest
+
+import dvbrx_b200 as D
+from helpers import check_frames, checker
+
+pytestmark = pytest.mark.gpu
+
+# (short, rate, constellation, Es/N0): all kernel classes, levelled and not
+CODES = [
+    (0, "3_5", "8PSK", 6.0),
+    (0, "2_3", "8PSK", 6.8),
+    (1, "1_2", "QPSK", 1.6),
+    (0, "9_10", "QPSK", 7.0),   # degree 30: one-frame kernel only
+    (1, "8_9", "QPSK", 6.9),    # degree 27
+    (0, "13_45", "QPSK", -0.6),
+    (1, "11_45", "QPSK", 0.2),
+]
+
+
+def make_batch(n, seed):
+    import torch
+    rng = np.random.default_rng(seed)
+    code = rng.integers(0, len(CODES), size=n).astype(np.int32)
+    llr = torch.zeros((n, 64800), dtype=torch.int8, device="cuda")
+    handles = []
+    for c, (short, rate, const, es) in enumerate(CODES):
+        h = D.Ldpc(D.fec_lookup(short, rate), rate)
+        handles.append(h)
+        rows = np.nonzero(code == c)[0]
+        if len(rows):
+            l, _, _ = h.generate(len(rows), es, seed=seed * 100 + c, constellation=const)
+            llr[torch.from_numpy(rows).cuda().long(), : h.N] = l
+    return code, llr, handles
+
+
+def test_mixed_batch_tilings_and_tuner():
+    import torch
+    n = 700
+    code, llr, handles = make_batch(n, 3)
+    mix = D.LdpcMix([(s, r) for s, r, _, _ in CODES])
+    out = torch.zeros((n, 7290), dtype=torch.uint8, device="cuda")
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    mix.plan(code, llr, out, it, ok, 30)
+
+    # expected: each code's frames decoded on their own
+    want_bits = {}
+    want_it = np.zeros(n, np.int32)
+    want_ok = np.zeros(n, np.uint8)
+    for c, h in enumerate(handles):
+        rows = np.nonzero(code == c)[0]
+        if not len(rows):
+            continue
+        sub = llr[torch.from_numpy(rows).cuda().long(), : h.N].contiguous()
+        b, i, o = h.decode_device(sub, 30)
+        torch.cuda.synchronize()
+        want_bits[c] = (rows, b.cpu().numpy())
+        want_it[rows] = i.cpu().numpy()
+        want_ok[rows] = o.cpu().numpy()
+
+    def check():
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        for c, (rows, b) in want_bits.items():
+            nb = handles[c].nbytes
+            assert (got[rows, :nb] == b).all(), CODES[c]
+        assert (it.cpu().numpy() == want_it).all()
+        assert (ok.cpu().numpy() == want_ok).all()
+
+    for tiling in (D.TILING_ONE_LAUNCH, D.TILING_PER_CODE):
+        out.zero_()
+        it.fill_(-1)
+        mix.set_tiling(tiling)
+        mix.run()
+        check()
+    choice, t1, t2 = mix.tune()
+    assert choice in (D.TILING_ONE_LAUNCH, D.TILING_PER_CODE) and t1 > 0 and t2 > 0
+    out.zero_()
+    mix.run()
+    check()
+
+    # a sample of frames against the reference decoder itself
+    for c, (short, rate, _, _) in enumerate(CODES[:3]):
+        rows = np.nonzero(code == c)[0][:3]
+        h = handles[c]
+        host = llr[torch.from_numpy(rows).cuda().long(), : h.N].cpu().numpy()
+        rb, ri, ro = check_frames(checker(short, rate), host, 30)
+        assert (out.cpu().numpy()[rows, : h.nbytes] == rb).all()
+        assert (it.cpu().numpy()[rows] == ri).all()
+    mix.close()

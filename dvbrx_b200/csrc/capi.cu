@@ -150,7 +150,9 @@ bool upload_code(drx_ldpc* d)
     const size_t o_eoff = o_ent + a16(c.ent.size() * sizeof(int32_t));
     const size_t o_steps = o_eoff + a16(c.eoff.size() * sizeof(uint16_t));
     const size_t o_perm = o_steps + a16(c.steps.size() * sizeof(uint32_t));
-    const size_t total = o_perm + a16(c.perm.size() * sizeof(uint16_t));
+    const size_t o_lmeta = o_perm + a16(c.perm.size() * sizeof(uint16_t));
+    const size_t o_nlev = o_lmeta + a16(c.lmeta.size() * sizeof(uint64_t));
+    const size_t total = o_nlev + a16(c.nlev.size());
     std::vector<char> host(total, 0);
     if (!cuda_ok(cudaMalloc(&d->blob, total), "cudaMalloc(code)"))
         return false;
@@ -169,7 +171,11 @@ bool upload_code(drx_ldpc* d)
     dc.eoff = (const uint16_t*)(base + o_eoff);
     dc.steps = (const uint32_t*)(base + o_steps);
     dc.perm = (const uint16_t*)(base + o_perm);
+    dc.lmeta = (const unsigned long long*)(base + o_lmeta);
+    dc.nlev = (const uint8_t*)(base + o_nlev);
     memcpy(host.data(), &dc, sizeof(dc));
+    memcpy(host.data() + o_lmeta, c.lmeta.data(), c.lmeta.size() * sizeof(uint64_t));
+    memcpy(host.data() + o_nlev, c.nlev.data(), c.nlev.size());
     memcpy(host.data() + o_ent, c.ent.data(), c.ent.size() * sizeof(int32_t));
     memcpy(host.data() + o_eoff, c.eoff.data(), c.eoff.size() * sizeof(uint16_t));
     memcpy(host.data() + o_steps, c.steps.data(), c.steps.size() * sizeof(uint32_t));
@@ -226,7 +232,7 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
             return -1;
         p.msg = d->msg;
         p.msg_stride = slab;
-        return cuda_ok(launch_decode_pair(p, d->code.dclass, d->pair_smem, grid, s), "decoder launch") ? 0 : -1;
+        return cuda_ok(launch_decode_pair(p, d->pair_kid, d->pair_smem, grid, s), "decoder launch") ? 0 : -1;
     }
     if (stop == 0) {
         grid = std::min(nframes, capacity);
@@ -321,10 +327,11 @@ drx_ldpc* drx_ldpc_new(const drx_fec_params* p, const char* rate)
         return nullptr;
     }
     d->ctas_per_sm = decode_ctas_per_sm(d->code.dclass, d->smem);
-    if (pair_supported(d->code.dclass)) {
+    d->pair_kid = pair_kernel_id(d->code);
+    if (d->pair_kid >= 0) {
         d->pair_smem = decode_pair_smem_bytes(d->code.N, (int)d->code.ent.size() / 2,
                                               (int)d->code.steps.size(), d->code.q);
-        d->pair_ctas_per_sm = decode_pair_ctas_per_sm(d->code.dclass, d->pair_smem);
+        d->pair_ctas_per_sm = decode_pair_ctas_per_sm(d->pair_kid, d->pair_smem);
     }
     if (d->ctas_per_sm <= 0) {
         set_err("decoder kernel does not fit on this device");

@@ -76,6 +76,7 @@ bool compile_code(int table, Code* c, std::string* err)
     c->ent.clear();
     c->eoff.assign(1, 0);
     c->cnt_max = 0;
+    c->cnt_min = 1 << 30;
     int info_links = 0;
     for (int i = 0; i < q; i++) {
         for (auto& e : layer[i]) {
@@ -84,6 +85,7 @@ bool compile_code(int table, Code* c, std::string* err)
         }
         c->eoff.push_back((uint16_t)(c->ent.size() / 2));
         c->cnt_max = std::max<int>(c->cnt_max, (int)layer[i].size());
+        c->cnt_min = std::min<int>(c->cnt_min, (int)layer[i].size());
         info_links += (int)layer[i].size() * QC;
     }
     c->deg_max = c->cnt_max + 2;
@@ -107,9 +109,32 @@ bool compile_code(int table, Code* c, std::string* err)
     /* levels inside each layer */
     c->steps.clear();
     c->perm.assign((size_t)q * QC, 0);
+    c->nlev.assign(q, 1);
+    c->lmeta.assign((size_t)q * QC, 0);
     c->levelled = false;
     c->nlevels = 0;
     for (int i = 0; i < q; i++) {
+        /* per check j: which of its information slots share their bit with
+         * an earlier (in) or a later (out) check of the layer */
+        const int ne = (int)layer[i].size();
+        for (int j = 0; j < QC; j++) {
+            uint64_t in = 0, out = 0;
+            for (int x = 0; x < ne; x++)
+                for (int y = 0; y < ne; y++) {
+                    if (x == y || layer[i][x].first != layer[i][y].first)
+                        continue;
+                    /* bit of slot x of check j is slot y's bit of check jp */
+                    const int jp = ((j - layer[i][x].second + layer[i][y].second) % QC + QC) % QC;
+                    if (jp < j)
+                        in |= 1ull << (2 + x);
+                    else if (jp > j)
+                        out |= 1ull << (2 + x);
+                }
+            /* masks of 24 slots: layers with more links (check degree
+             * above 24) keep none; the phased schedule does not run them */
+            if (2 + ne <= 24)
+                c->lmeta[(size_t)i * QC + j] = in << 8 | out << 32;
+        }
         std::vector<int> offs; /* d: check j shares a bit with check (j + d) mod 360 */
         for (size_t x = 0; x < layer[i].size(); x++)
             for (size_t y = 0; y < layer[i].size(); y++)
@@ -131,6 +156,9 @@ bool compile_code(int table, Code* c, std::string* err)
         }
         const bool perm = nl > 1;
         c->levelled |= perm;
+        c->nlev[i] = (uint8_t)nl;
+        for (int j = 0; j < QC; j++)
+            c->lmeta[(size_t)i * QC + j] |= (uint64_t)lev[j];
         int pos = 0;
         for (int l = 0; l < nl; l++) {
             const int start = pos;

@@ -33,6 +33,7 @@ struct Code {
     std::string table_name; /* e.g. "DVB_S2_TABLE_B5" */
     int N = 0, K = 0, R = 0, q = 0;
     int cnt_max = 0;   /* most information links of a check */
+    int cnt_min = 0;   /* fewest information links of a layer */
     int deg_max = 0;   /* cnt_max + 2 parity links */
     int dclass = 0;    /* kernel class: degree_class(deg_max) */
     int edges = 0;     /* links of the whole Tanner graph */
@@ -47,6 +48,14 @@ struct Code {
     std::vector<uint32_t> steps;
     /* q * 360 check indexes by position (identity for unlevelled layers) */
     std::vector<uint16_t> perm;
+    /* per layer: number of wavefront levels */
+    std::vector<uint8_t> nlev;
+    /* per check j of layer i (index 360 i + j), for the phased schedule:
+     * bits 0-7 its level, bits 8-31 the link slots it reads after an earlier
+     * check of the layer wrote them ("in"), bits 32-55 the slots a later
+     * check of the layer reads after it ("out").  Slot 0 = parity, 1 =
+     * previous parity, 2 + e = information entry e of the layer. */
+    std::vector<uint64_t> lmeta;
     /* accumulator addresses of the standard table, for the encoder:
      * per information bit group g, addr[aoff[g] .. aoff[g+1]-1] */
     std::vector<uint16_t> addr;
@@ -58,6 +67,9 @@ struct Code {
  * the codes it runs. */
 constexpr int kNumClasses = 6;
 constexpr int kClassDeg[kNumClasses] = { 7, 11, 14, 18, 22, 32 };
+/* smallest information-link count of a layer in the codes of each class
+ * (the frame-pair kernel instantiates link counts kClassCntLo .. max) */
+constexpr int kClassCntLo[kNumClasses] = { 1, 5, 7, 12, 14, 25 };
 int degree_class(int deg_max);
 
 /* Rate string -> table index (cg_rates_normal / cg_rates_short), or -1.

@@ -26,6 +26,7 @@ struct drx_ldpc {
     int ctas_per_sm = 0;
     size_t pair_smem = 0;
     int pair_ctas_per_sm = 0; /* 0: the frame-pair kernel does not run this code */
+    int pair_kid = -1;        /* its instantiation for this code */
     int variant = DRX_VARIANT_AUTO;
     cudaStream_t stream = nullptr;
     /* scratch */

@@ -19,6 +19,8 @@ struct DevCode {
     const uint16_t* eoff;  /* q + 1 */
     const uint32_t* steps; /* nsteps: layer | start << 8 | count << 17 | perm << 26 */
     const uint16_t* perm;  /* q * 360 */
+    const uint8_t* nlev;   /* q: wavefront levels of each layer */
+    const unsigned long long* lmeta; /* q * 360: level | in slots << 8 | out slots << 32 */
 };
 
 /* Work of one launch of the plain decoder. */
@@ -86,11 +88,13 @@ cudaError_t launch_decode(const DecodeParams& p, int dclass, size_t smem, int gr
 namespace drxg {
 
 /* Frame-pair variant (ldpc_pair.cu): two frames per CTA in 16x2 SIMD, codes
- * up to check degree 16; per-frame stopping only. */
-bool pair_supported(int dclass);
+ * up to check degree 14; per-frame stopping only.  pair_kernel_id picks the
+ * instantiation for a code (-1: not run by the frame-pair kernel). */
+struct Code;
+int pair_kernel_id(const Code& c);
 size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q);
 size_t decode_pair_msg_bytes(int R);
-int decode_pair_ctas_per_sm(int dclass, size_t smem);
-cudaError_t launch_decode_pair(const DecodeParams& p, int dclass, size_t smem, int grid, cudaStream_t stream);
+int decode_pair_ctas_per_sm(int kid, size_t smem);
+cudaError_t launch_decode_pair(const DecodeParams& p, int kid, size_t smem, int grid, cudaStream_t stream);
 
 }  // namespace drxg

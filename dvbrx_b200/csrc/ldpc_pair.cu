@@ -14,21 +14,20 @@
  * v holds the int8 posterior of variable v for lane A (low byte) and lane B
  * (high byte): K information bits, then R parity bits in layer order.
  *
- * A check node is spread over L lanes of a warp (its links c = r, r + L, ...
- * go to lane r): L = 2 on the full 360-check steps, L = 4 or 8 on the small
- * steps of levelled layers, so that the serial part of a step (a check
- * node's chain over its links) is short where few checks can run.  The
- * lanes combine their two smallest magnitudes and sign parities with
- * shuffles, then each writes its own links' outputs; the group's first lane
- * stores the check's compressed messages for both frames in one 8-byte
- * record: per lane min0 (6 bits) | min1 << 6 | index << 12, then the sign
- * bits of lane A in the low half and of lane B in the high half.
+ * A check node runs on two threads (its links alternate between them), which
+ * combine their two smallest magnitudes and sign parities with one shuffle
+ * round; 720 of the 768 threads hold the 360 checks of a layer.  Levelled
+ * layers run in phases (layer_pair): the wavefront levels carry only the
+ * links two checks of the layer share.  The first thread of a check stores
+ * its compressed messages for both frames in one 8-byte record: per lane
+ * min0 (6 bits) | min1 << 6 | index << 12, then the sign bits of lane A in
+ * the low half and of lane B in the high half.
  *
  * Frames stream through the two lanes independently: when a lane's frame
  * passes the syndrome check or reaches max_iter, its results are written
  * and the lane takes the next frame of the batch (its first iteration reads
  * zero messages), so a converged frame never waits for its neighbour.
- * Codes up to check degree 16 (degree classes 0-2) run here.
+ * Codes up to check degree 14 (degree classes 0-2) run here.
  */
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -73,137 +72,143 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
 }
 
 /*
- * Check node (i, j) for both lanes, spread over L threads (lane r of the
- * group).  Slots: 0 = parity bit, 1 = previous parity bit (absent for
- * (0, 0)), 2.. = information bits.
+ * One check node (i, j) for both lanes, on two threads (r = 0, 1): thread r
+ * owns the node's link slots c = r, r + 2, ...  Slot 0 is the parity bit,
+ * slot 1 the previous parity bit (absent for (0, 0)), 2 + e information
+ * entry e of the layer.  DM is the node degree (EXACT) or a bound on it
+ * (the degree is then a run-time value and slots past it are skipped).
+ * The node state lives in registers across the phases of its layer (see
+ * layer_pair).  The message's sign bits and index are shifted by r once, so
+ * that everything a slot needs besides its address depends on k alone.
  */
-template <int CNT, int L>
-__device__ __forceinline__ void check_pair(uint16_t* __restrict__ post, const int2* __restrict__ ent,
-                                           int K, int q, int i, int j, int r, uint2 rec, uint32_t fresh,
-                                           unsigned gmask, uint2* __restrict__ dst)
-{
-    constexpr int D = CNT + 2;
-    constexpr int S = (D + L - 1) / L;
-    const bool has_pp = (i | j) != 0;
-    const int pc = K + kQCp * i + j;
-    const int pp = i ? pc - kQCp : K + kQCp * (q - 1) + j - 1;
-
-    /* this lane's slots: c = r + k L */
+template <int DM, bool EXACT>
+struct PairCheck {
+    static constexpr int S = (DM + 1) / 2;
+    int D;
+    int r;
     int addr[S];
-    bool live[S];
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-        const int c = r + k * L;
-        live[k] = c < D && (c != 1 || has_pp);
-        int a = 0;
-        if (k == 0 && L > 2) {
-            a = c == 0 ? pc : c == 1 ? pp : 0;
-        } else if (k == 0) {
-            a = r == 0 ? pc : pp; /* L <= 2: slot r is a parity slot */
-        }
-        const bool info = (k > 0) || (c >= 2);
-        if (info && c < D) {
-            const int2 e = ent[c - 2];
-            a = e.x + j + (j < e.y ? kQCp : 0);
-        }
-        addr[k] = a;
-    }
-    /* messages of the check: zero for a lane in its first iteration */
-    const uint32_t w0 = rec.x & ~fresh, sgn = rec.y & ~fresh;
-    const uint32_t m0 = w0 & 0x003F003Fu, m1 = (w0 >> 6) & 0x003F003Fu;
-    const uint32_t idxh = ((w0 >> 12) & 0x000F000Fu) | 0x64006400u; /* FP16 1024 + index */
-    /* minus the message: +m if it is negative, else -min(m, 31) */
-    const uint32_t n0 = m0, n1 = m1;
-    const uint32_t p0 = neg2(__vmins2(m0, 0x001F001Fu)), p1 = neg2(__vmins2(m1, 0x001F001Fu));
-
     uint32_t x[S];
-    uint32_t min0 = 0x00FF00FFu, min1 = 0x00FF00FFu, sg = 0;
+    uint32_t livem; /* bit k: owned slot k is a link of this node */
+    uint32_t n0, n1, p0, p1, idxh, sgn;
+    uint32_t min0, min1, sg, mn0, mn1, min0p1;
+    uint32_t inm, outm; /* bit k: owned slot k is read late / written early */
+
+    __device__ __forceinline__ void setup(const int2* __restrict__ ent, int cnt, int K, int q, int i, int j,
+                                          int rr, uint2 rec, uint32_t fresh, unsigned long long meta)
+    {
+        r = rr;
+        D = EXACT ? DM : cnt + 2;
+        const bool has_pp = (i | j) != 0;
+        const int pc = K + kQCp * i + j;
+        const int pp = i ? pc - kQCp : K + kQCp * (q - 1) + j - 1;
+        const uint32_t in24 = (uint32_t)(meta >> 8) & 0xFFFFFFu, out24 = (uint32_t)(meta >> 32) & 0xFFFFFFu;
+        livem = inm = outm = 0;
 #pragma unroll
-    for (int k = 0; k < S; k++) {
-        const int c = r + k * L;
-        uint32_t v = 0x00FF00FFu; /* absent link: 255 in both lanes */
-        if (live[k]) {
-            v = sx2(post[addr[k]]);
-            const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)c * 0x00010001u);
-            const uint32_t sm = lmask(sgn << (15 - c));
-            const uint32_t nm = sel(sm, sel(im, n1, n0), sel(im, p1, p0));
-            v = sadd(v, nm);
+        for (int k = 0; k < S; k++) {
+            const int c = r + 2 * k;
+            int a = r == 0 ? pc : pp;
+            if (k > 0 && c < D) {
+                const int2 e = ent[c - 2];
+                a = e.x + j + (j < e.y ? kQCp : 0);
+            }
+            addr[k] = a;
+            if (c < D && (c != 1 || has_pp))
+                livem |= 1u << k;
+            inm |= ((in24 >> c) & 1u) << k;
+            outm |= ((out24 >> c) & 1u) << k;
+            x[k] = 0x00FF00FFu; /* absent link: 255 in both lanes, positive */
         }
-        x[k] = v;
-        const uint32_t a = abs2(v);
-        min1 = __vmins2(min1, __vmaxs2(min0, a));
-        min0 = __vmins2(min0, a);
-        sg ^= v;
+        /* messages: zero for a lane in its first iteration */
+        const uint32_t w0 = rec.x & ~fresh;
+        sgn = (rec.y & ~fresh) >> r;
+        const uint32_t m0 = w0 & 0x003F003Fu, m1 = (w0 >> 6) & 0x003F003Fu;
+        idxh = (((w0 >> 12) & 0x000F000Fu) | 0x64006400u) - (uint32_t)r * 0x00010001u; /* FP16 1024 + index - r */
+        /* minus the message: +m if it is negative, else -min(m, 31) */
+        n0 = m0;
+        n1 = m1;
+        p0 = neg2(__vmins2(m0, 0x001F001Fu));
+        p1 = neg2(__vmins2(m1, 0x001F001Fu));
+        min0 = min1 = 0x00FF00FFu;
+        sg = 0;
     }
+
+    /* extrinsic inputs of the owned slots that are (in_pass) or are not
+     * written earlier in the layer, folded into this thread's partial
+     * minimums and sign parity */
+    __device__ __forceinline__ void read(const uint16_t* __restrict__ post, bool in_pass)
+    {
 #pragma unroll
-    for (int o = 1; o < L; o <<= 1) {
-        const uint32_t b0 = __shfl_xor_sync(gmask, min0, o);
-        const uint32_t b1 = __shfl_xor_sync(gmask, min1, o);
-        const uint32_t bs = __shfl_xor_sync(gmask, sg, o);
+        for (int k = 0; k < S; k++) {
+            if (!((livem >> k) & 1) || (((inm >> k) & 1) != 0) != in_pass)
+                continue;
+            uint32_t v = sx2(post[addr[k]]);
+            const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(2 * k) * 0x00010001u);
+            const uint32_t sm = lmask(sgn << (15 - 2 * k));
+            v = sadd(v, sel(sm, sel(im, n1, n0), sel(im, p1, p0)));
+            x[k] = v;
+            const uint32_t a = abs2(v);
+            min1 = __vmins2(min1, __vmaxs2(min0, a));
+            min0 = __vmins2(min0, a);
+            sg ^= v;
+        }
+    }
+
+    /* combine with the partner thread; offset 1 and the cap at 127 */
+    __device__ __forceinline__ void finish(unsigned gmask)
+    {
+        const uint32_t b0 = __shfl_xor_sync(gmask, min0, 1);
+        const uint32_t b1 = __shfl_xor_sync(gmask, min1, 1);
+        const uint32_t bs = __shfl_xor_sync(gmask, sg, 1);
         min1 = __vmins2(__vmaxs2(min0, b0), __vmins2(min1, b1));
         min0 = __vmins2(min0, b0);
         sg ^= bs;
+        mn0 = __viaddmax_s16x2(__vmins2(min0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+        mn1 = __viaddmax_s16x2(__vmins2(min1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+        min0p1 = __vadd2(min0, 0x00010001u);
     }
-    /* offset 1 and the cap at 127, once per node */
-    const uint32_t mn0 = __viaddmax_s16x2(__vmins2(min0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
-    const uint32_t mn1 = __viaddmax_s16x2(__vmins2(min1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
-    const uint32_t min0p1 = __vadd2(min0, 0x00010001u);
-    uint32_t nidx = 0, nsg = 0;
+
+    /* new posteriors of the owned slots that are (out_pass) or are not read
+     * by a later check of the layer */
+    __device__ __forceinline__ void write(uint16_t* __restrict__ post, bool out_pass)
+    {
 #pragma unroll
-    for (int k = 0; k < S; k++) {
-        const int c = r + k * L;
-        const uint32_t v = x[k];
-        const uint32_t eq = lmask(__vsub2(abs2(v), min0p1)); /* |x| == min0 */
-        const uint32_t mag = sel(eq, mn1, mn0);
-        const uint32_t sm = lmask(sg ^ v);
-        const uint32_t o = __vsub2(mag ^ sm, sm);
-        if (live[k])
+        for (int k = 0; k < S; k++) {
+            if (!((livem >> k) & 1) || (((outm >> k) & 1) != 0) != out_pass)
+                continue;
+            const uint32_t v = x[k];
+            const uint32_t eq = lmask(__vsub2(abs2(v), min0p1)); /* |x| == min0 */
+            const uint32_t sm = lmask(sg ^ v);
+            const uint32_t o = __vsub2(sel(eq, mn1, mn0) ^ sm, sm);
             post[addr[k]] = (uint16_t)pk2(sadd(v, o));
-        if (c < D) {
-            nidx = sel(eq, (uint32_t)c * 0x00010001u, nidx);
-            nsg |= sm & (0x00010001u << c);
         }
     }
+
+    /* the node's compressed messages for both lanes, stored by thread 0:
+     * the slot holding min0 and one sign bit per slot */
+    __device__ __forceinline__ void record(unsigned gmask, uint2* __restrict__ dst)
+    {
+        uint32_t nidx = 0, nsg = 0; /* nidx per lane: 2k + 1 of an owned slot holding min0, 0 if none */
 #pragma unroll
-    for (int o = 1; o < L; o <<= 1) {
-        nidx = __vmaxs2(nidx, __shfl_xor_sync(gmask, nidx, o));
-        nsg |= __shfl_xor_sync(gmask, nsg, o);
+        for (int k = 0; k < S; k++) {
+            if (r + 2 * k >= D)
+                continue;
+            const uint32_t v = x[k];
+            const uint32_t eq = lmask(__vsub2(abs2(v), min0p1));
+            nidx = sel(eq, (uint32_t)(2 * k + 1) * 0x00010001u, nidx);
+            nsg |= lmask(sg ^ v) & (0x00010001u << (2 * k));
+        }
+        nsg <<= r; /* bit 2k -> slot 2k + r (slots stay below 16: no carry across lanes) */
+        const uint32_t found = lmask(__vsub2(0u, nidx)); /* lanes with nidx > 0 */
+        nidx = __vadd2(nidx, found & ((uint32_t)r * 0x00010001u)); /* 2k + r + 1 */
+        nidx = __vmaxs2(nidx, __shfl_xor_sync(gmask, nidx, 1));
+        nidx = __vmaxs2(__vsub2(nidx, 0x00010001u), 0u); /* slot number */
+        nsg |= __shfl_xor_sync(gmask, nsg, 1);
+        if (r == 0) {
+            const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
+            __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
+        }
     }
-    if (r == 0) {
-        const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
-        __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
-    }
-}
-
-template <int DMAX>
-struct PairLanes {
-    static constexpr int part = DMAX <= 8 ? 4 : 8; /* lanes per check on small steps */
 };
-
-template <int DMAX>
-__device__ __forceinline__ void check_pair_dispatch(int cnt, int L, uint16_t* post, const int2* ent, int K,
-                                                    int q, int i, int j, int r, uint2 rec, uint32_t fresh,
-                                                    unsigned gmask, uint2* dst)
-{
-    constexpr int LP = PairLanes<DMAX>::part;
-#define DRXG_PCASE(n)                                                                                \
-    case n:                                                                                          \
-        if (n + 2 <= DMAX) {                                                                         \
-            if (L == 2)                                                                              \
-                check_pair<(n + 2 <= DMAX ? n : 1), 2>(post, ent, K, q, i, j, r, rec, fresh, gmask, dst); \
-            else                                                                                     \
-                check_pair<(n + 2 <= DMAX ? n : 1), LP>(post, ent, K, q, i, j, r, rec, fresh, gmask, dst); \
-        }                                                                                            \
-        break;
-    switch (cnt) {
-        DRXG_PCASE(1) DRXG_PCASE(2) DRXG_PCASE(3) DRXG_PCASE(4) DRXG_PCASE(5) DRXG_PCASE(6)
-        DRXG_PCASE(7) DRXG_PCASE(8) DRXG_PCASE(9) DRXG_PCASE(10) DRXG_PCASE(11) DRXG_PCASE(12)
-        DRXG_PCASE(13) DRXG_PCASE(14)
-    default:
-        break;
-    }
-#undef DRXG_PCASE
-}
 
 struct PairFrame {
     uint16_t* post;
@@ -313,42 +318,84 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
     return r;
 }
 
-template <int DMAX>
+/*
+ * Layer i of the phased schedule.  Every check reads its links that no
+ * earlier check of the layer writes (a full-occupancy pass); then, level by
+ * level, the checks of the level read their remaining links (written by
+ * earlier levels), finish their minimums and write only the posteriors that
+ * later checks of the layer read; a last full pass writes every other
+ * posterior and the messages.  The reference's in-order semantics only
+ * constrain the bits two checks of a layer share, so the wavefront levels
+ * carry just those links.  Unlevelled layers take one pass.
+ */
+template <int DM, bool EXACT>
+__device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev, uint2 rec,
+                                           unsigned long long meta, uint32_t fresh, uint2* __restrict__ msg)
+{
+    const int t = threadIdx.x;
+    const bool active = t < 2 * kQCp;
+    const int j = t >> 1;
+    PairCheck<DM, EXACT> ck;
+    if (active) {
+        ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, t & 1, rec, fresh, meta);
+        ck.read(fr.post, false);
+    }
+    if (nlev > 1) {
+        const int lev = (int)(meta & 0xFF);
+        for (int l = 0; l < nlev; l++) {
+            const bool mine = active && lev == l;
+            const unsigned gm = __ballot_sync(0xFFFFFFFFu, mine);
+            if (mine) {
+                ck.read(fr.post, true);
+                ck.finish(gm);
+                ck.write(fr.post, true);
+            }
+            __syncthreads();
+        }
+    } else {
+        const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
+        if (active)
+            ck.finish(gm);
+    }
+    const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
+    if (active) {
+        ck.write(fr.post, false);
+        ck.record(gm, msg + kQCp * i + j);
+    }
+    __syncthreads();
+}
+
+/* One decoding iteration: the layers in order; each layer's messages and
+ * level metadata are fetched one layer ahead.  The kernel is compiled for
+ * the two information-link counts A <= B of its codes (exact-degree check
+ * nodes), or, with GDM > 0, for any count up to GDM - 2 (predicated). */
+template <int A, int B, int GDM>
 __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __restrict__ msg, uint32_t fresh)
 {
-    constexpr int LP = PairLanes<DMAX>::part;
     const int t = threadIdx.x;
-    auto lanes = [&](int n) { return n * LP <= (int)blockDim.x ? LP : 2; };
+    const int j = t >> 1;
+    const bool active = t < 2 * kQCp;
     uint2 rn = make_uint2(0, 0);
-    int jn = 0;
-    auto fetch = [&](int s, uint2& rec, int& jj) {
-        const uint32_t st = fr.steps[s];
-        const int i = st & 0xFF, start = (st >> 8) & 0x1FF, n = (st >> 17) & 0x1FF;
-        const int L = lanes(n);
-        const int g = t / L;
-        if (g < n) {
-            const int pos = start + g;
-            jj = (st >> 26) ? (int)__ldg(c.perm + kQCp * i + pos) : pos;
-            rec = __ldcg(msg + kQCp * i + pos);
-        }
-    };
-    fetch(0, rn, jn);
-    for (int s = 0; s < c.nsteps; s++) {
+    unsigned long long mn = 0;
+    if (active) {
+        rn = __ldcg(msg + j);
+        mn = __ldg(c.lmeta + j);
+    }
+    for (int i = 0; i < c.q; i++) {
         const uint2 rec = rn;
-        const int j = jn;
-        const uint32_t st = fr.steps[s];
-        const int i = st & 0xFF, start = (st >> 8) & 0x1FF, n = (st >> 17) & 0x1FF;
-        if (s + 1 < c.nsteps)
-            fetch(s + 1, rn, jn);
-        const int L = lanes(n);
-        const int g = t / L, r = t % L;
-        const unsigned gmask = __ballot_sync(0xFFFFFFFFu, g < n);
-        if (g < n) {
-            const int e0 = fr.eoff[i];
-            check_pair_dispatch<DMAX>(fr.eoff[i + 1] - e0, L, fr.post, fr.ent + e0, c.K, c.q, i, j, r, rec,
-                                      fresh, gmask, msg + kQCp * i + start + g);
+        const unsigned long long meta = mn;
+        if (active && i + 1 < c.q) {
+            rn = __ldcg(msg + kQCp * (i + 1) + j);
+            mn = __ldg(c.lmeta + kQCp * (i + 1) + j);
         }
-        __syncthreads();
+        const int cnt = fr.eoff[i + 1] - fr.eoff[i];
+        const int nlev = c.nlev[i];
+        if (GDM > 0)
+            layer_pair<(GDM > 0 ? GDM : 2), false>(fr, c, i, cnt, nlev, rec, meta, fresh, msg);
+        else if (A == B || cnt == A)
+            layer_pair<A + 2, true>(fr, c, i, cnt, nlev, rec, meta, fresh, msg);
+        else
+            layer_pair<B + 2, true>(fr, c, i, cnt, nlev, rec, meta, fresh, msg);
     }
 }
 
@@ -367,8 +414,8 @@ __device__ void store_lane(const DevCode& c, const PairFrame& fr, int h, uint8_t
     }
 }
 
-template <int DMAX, int MINB>
-__global__ void __launch_bounds__(kPT, MINB) k_decode_pair(DecodeParams p)
+template <int A, int B, int GDM>
+__global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
 {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_frame[2], s_iter[2], s_flag, s_reload;
@@ -434,7 +481,7 @@ __global__ void __launch_bounds__(kPT, MINB) k_decode_pair(DecodeParams p)
         __syncthreads();
         if (done)
             continue; /* reload, then check the new frames first */
-        iterate_pair<DMAX>(c, fr, msg, fresh);
+        iterate_pair<A, B, GDM>(c, fr, msg, fresh);
         fresh = 0;
         if (t == 0) {
             s_iter[0]++;
@@ -453,25 +500,55 @@ size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q)
 
 size_t decode_pair_msg_bytes(int R) { return (size_t)R * sizeof(uint2); }
 
-bool pair_supported(int dclass) { return dclass >= 0 && dclass <= 2; }
+/* Pair kernels by information-link counts (A, B): every pair of the DVB-S2,
+ * S2X and T2 codes up to check degree 14, plus predicated kernels for the
+ * codes whose layers have more than two different counts. */
+struct PairKernel {
+    int a, b, gdm;
+    const void* fn;
+};
 
-static const void* pair_kernel(int dclass)
+#define DRXG_PK(a, b) { a, b, 0, (const void*)k_decode_pair<a, b, 0> }
+#define DRXG_PG(d) { 0, 0, d, (const void*)k_decode_pair<1, 1, d> }
+static const PairKernel kPairKernels[] = {
+    DRXG_PK(1, 2), DRXG_PK(2, 2), DRXG_PK(2, 3), DRXG_PK(3, 3), DRXG_PK(4, 4), DRXG_PK(5, 5),
+    DRXG_PK(5, 6), DRXG_PK(6, 7), DRXG_PK(7, 7), DRXG_PK(7, 8), DRXG_PK(8, 8), DRXG_PK(8, 9),
+    DRXG_PK(9, 9), DRXG_PK(9, 10), DRXG_PK(11, 11), DRXG_PK(11, 12), DRXG_PK(12, 12),
+    DRXG_PG(7), DRXG_PG(11), DRXG_PG(14),
+};
+#undef DRXG_PK
+#undef DRXG_PG
+constexpr int kNumPairKernels = (int)(sizeof(kPairKernels) / sizeof(kPairKernels[0]));
+
+int pair_kernel_id(const Code& c)
 {
-    switch (dclass) {
-    case 0:
-        return (const void*)k_decode_pair<7, 1>;
-    case 1:
-        return (const void*)k_decode_pair<11, 1>;
-    default:
-        return (const void*)k_decode_pair<14, 1>;
+    if (c.deg_max > 14)
+        return -1;
+    int lo = 1 << 30, hi = 0, other = 0;
+    for (int i = 0; i < c.q; i++) {
+        const int n = c.eoff[i + 1] - c.eoff[i];
+        lo = n < lo ? n : lo;
+        hi = n > hi ? n : hi;
     }
+    for (int i = 0; i < c.q; i++) {
+        const int n = c.eoff[i + 1] - c.eoff[i];
+        other |= n != lo && n != hi;
+    }
+    if (!other)
+        for (int k = 0; k < kNumPairKernels; k++)
+            if (kPairKernels[k].gdm == 0 && kPairKernels[k].a == lo && kPairKernels[k].b == hi)
+                return k;
+    for (int k = 0; k < kNumPairKernels; k++)
+        if (kPairKernels[k].gdm >= c.deg_max)
+            return k;
+    return -1;
 }
 
-int decode_pair_ctas_per_sm(int dclass, size_t smem)
+int decode_pair_ctas_per_sm(int kid, size_t smem)
 {
-    if (!pair_supported(dclass))
+    if (kid < 0 || kid >= kNumPairKernels)
         return 0;
-    const void* k = pair_kernel(dclass);
+    const void* k = kPairKernels[kid].fn;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 0;
     int n = 0;
@@ -480,11 +557,11 @@ int decode_pair_ctas_per_sm(int dclass, size_t smem)
     return n;
 }
 
-cudaError_t launch_decode_pair(const DecodeParams& p, int dclass, size_t smem, int grid, cudaStream_t stream)
+cudaError_t launch_decode_pair(const DecodeParams& p, int kid, size_t smem, int grid, cudaStream_t stream)
 {
-    if (!pair_supported(dclass))
+    if (kid < 0 || kid >= kNumPairKernels)
         return cudaErrorInvalidValue;
-    const void* k = pair_kernel(dclass);
+    const void* k = kPairKernels[kid].fn;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;

@@ -245,7 +245,7 @@ int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const i
     for (auto* h : m->codes) {
         decode_ctas_per_sm(h->code.dclass, h->smem);
         if (h->pair_ctas_per_sm > 0)
-            decode_pair_ctas_per_sm(h->code.dclass, h->pair_smem);
+            decode_pair_ctas_per_sm(h->pair_kid, h->pair_smem);
     }
 
     for (int t = DRX_TILING_ONE_LAUNCH; t <= DRX_TILING_PER_CODE; t++) {
@@ -300,7 +300,7 @@ int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const i
                 p.msg_stride = code_slab[c];
                 e = cudaMemsetAsync(p.work, 0, sizeof(unsigned), s);
                 if (e == cudaSuccess)
-                    e = pair_runs(h) ? launch_decode_pair(p, h->code.dclass, h->pair_smem, code_grid[c], s)
+                    e = pair_runs(h) ? launch_decode_pair(p, h->pair_kid, h->pair_smem, code_grid[c], s)
                                      : launch_decode(p, h->code.dclass, h->smem, code_grid[c], s);
             }
             for (int s = 0; s < kSideStreams; s++) {

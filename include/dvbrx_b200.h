@@ -181,6 +181,46 @@ int drx_ldpc_mix_tune(drx_ldpc_mix* m, void* stream, float* ms_one_launch, float
 /* Launch the plan's graph (the tuned or set tiling) on `stream`. */
 int drx_ldpc_mix_run(drx_ldpc_mix* m, void* stream);
 
+/* ---- learned (neural offset / scaled) min-sum: training -------------------
+ *
+ * The plain decoder's layered schedule with the check node's offset 1
+ * replaced by mag = max(beta[t][k] * min(min_other, 127) - alpha[t][k], 0)
+ * for iteration t and check-degree class k (class_of_degree[D], D = 0..32),
+ * with the int8 decoder's saturations, in fp32 on the int8 scale (2 x LLR).
+ * Loss: sum over iterations and information bits of the binary
+ * cross-entropy softplus(-(1 - 2 b) P / 2) of the posterior P after each
+ * iteration.  Parameters are FP16 (iters x nclass), inputs FP16 LLRs
+ * (unquantised, 2 x LLR), targets the packed information bits.  The caller
+ * owns all memory; nothing is allocated. */
+size_t drx_learned_workspace_bytes(const drx_ldpc* d, int nframes, int iters, int train);
+
+/* Forward over nframes frames; loss[t] (device, zeroed by the caller)
+ * receives the BCE sum after iteration t; post (device, optional) the final
+ * posteriors of the kldpc information bits.  With train != 0 the
+ * workspace keeps one checkpoint per iteration for drx_learned_backward. */
+int drx_learned_forward(drx_ldpc* d, int nframes, const void* llr_f16, size_t llr_stride, const uint8_t* bits,
+                        size_t bits_stride, int iters, const void* beta_f16, const void* alpha_f16, int nclass,
+                        const int8_t* class_of_degree, float* loss, float* post, void* workspace,
+                        size_t workspace_bytes, int train, void* stream);
+
+/* Backward of a training forward with the same arguments and workspace:
+ * adds to dbeta and dalpha (device fp32, iters x nclass) the gradient of
+ * loss_scale x (sum of the per-iteration BCE sums).  loss_scratch: device
+ * float[iters] the re-run forward writes into. */
+int drx_learned_backward(drx_ldpc* d, int nframes, const void* llr_f16, size_t llr_stride, const uint8_t* bits,
+                         size_t bits_stride, int iters, const void* beta_f16, const void* alpha_f16, int nclass,
+                         const int8_t* class_of_degree, float loss_scale, float* dbeta, float* dalpha,
+                         float* loss_scratch, void* workspace, size_t workspace_bytes, void* stream);
+
+/* The decoding schedule of a code, computed on the host: the number of
+ * steps and the largest check degree; for every check (layer-order index
+ * 360 i + j) its step (check_step[R]) and its links (links[R][deg_max]:
+ * parity bit, previous parity bit or -1, information bits, -1 padding) as
+ * codeword bit indexes (parity bit of check q j + i at K + q j + i).
+ * Either array may be NULL. */
+int drx_ldpc_schedule(int short_frame, const char* rate, int* nsteps, int* deg_max, int32_t* check_step,
+                      int32_t* links);
+
 /* Device error word of the handle: 0, or the code of a device-side fault
  * report (2: a group barrier timed out).  Cleared by the call. */
 int drx_ldpc_device_error(drx_ldpc* d);

@@ -73,50 +73,55 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
 
 /*
  * One check node (i, j) for both lanes, on two threads (r = 0, 1): thread r
- * owns the node's link slots c = r, r + 2, ...  Slot 0 is the parity bit,
- * slot 1 the previous parity bit (absent for (0, 0)), 2 + e information
- * entry e of the layer.  DM is the node degree (EXACT) or a bound on it
- * (the degree is then a run-time value and slots past it are skipped).
- * The node state lives in registers across the phases of its layer (see
- * layer_pair).  The message's sign bits and index are shifted by r once, so
- * that everything a slot needs besides its address depends on k alone.
+ * owns the node's link slots c = r + 2k, k = 0 .. S-1.  Slot 0 is the
+ * parity bit, slot 1 the previous parity bit (absent for (0, 0)), 2 + e
+ * information entry e of the layer.  DM is the node degree (EXACT) or a
+ * bound on it (the degree is then a run-time value).  The node state lives
+ * in registers across the phases of its layer (see layer_pair).
+ *
+ * Slot masks keep owned slot k at bit 2k (the layer's 24-bit slot masks
+ * shifted right by r); the message's sign bits and index are shifted by r
+ * the same way, so everything a slot needs besides its address depends on
+ * k alone.  The full passes run every slot without branches: a slot that is
+ * not a link, or whose bit an earlier check of the layer writes (read later,
+ * in its level), enters the minimums as 255, which no magnitude reaches;
+ * stores are predicated.
  */
 template <int DM, bool EXACT>
 struct PairCheck {
     static constexpr int S = (DM + 1) / 2;
-    int D;
     int r;
     int addr[S];
     uint32_t x[S];
-    uint32_t livem; /* bit k: owned slot k is a link of this node */
+    uint32_t live, inm, outm; /* bit 2k: owned slot k is a link / is read late / is written early */
     uint32_t n0, n1, p0, p1, idxh, sgn;
-    uint32_t min0, min1, sg, mn0, mn1, min0p1;
-    uint32_t inm, outm; /* bit k: owned slot k is read late / written early */
+    uint32_t min0, min1, sg, mn0, mn1;
 
     __device__ __forceinline__ void setup(const int2* __restrict__ ent, int cnt, int K, int q, int i, int j,
                                           int rr, uint2 rec, uint32_t fresh, unsigned long long meta)
     {
         r = rr;
-        D = EXACT ? DM : cnt + 2;
-        const bool has_pp = (i | j) != 0;
+        const int D = EXACT ? DM : cnt + 2;
         const int pc = K + kQCp * i + j;
         const int pp = i ? pc - kQCp : K + kQCp * (q - 1) + j - 1;
-        const uint32_t in24 = (uint32_t)(meta >> 8) & 0xFFFFFFu, out24 = (uint32_t)(meta >> 32) & 0xFFFFFFu;
-        livem = inm = outm = 0;
+        uint32_t lv = (1u << D) - 1u;
+        if ((i | j) == 0)
+            lv &= ~2u;
+        live = lv >> r;
+        inm = ((uint32_t)(meta >> 8) & 0xFFFFFFu) >> r;
+        outm = ((uint32_t)(meta >> 32) & 0xFFFFFFu) >> r;
 #pragma unroll
         for (int k = 0; k < S; k++) {
             const int c = r + 2 * k;
-            int a = r == 0 ? pc : pp;
-            if (k > 0 && c < D) {
-                const int2 e = ent[c - 2];
+            int a;
+            if (k == 0) {
+                a = r == 0 ? pc : pp;
+            } else {
+                /* a slot past the degree takes the last link's address: read, never used */
+                const int2 e = ent[min(c, D - 1) - 2];
                 a = e.x + j + (j < e.y ? kQCp : 0);
             }
             addr[k] = a;
-            if (c < D && (c != 1 || has_pp))
-                livem |= 1u << k;
-            inm |= ((in24 >> c) & 1u) << k;
-            outm |= ((out24 >> c) & 1u) << k;
-            x[k] = 0x00FF00FFu; /* absent link: 255 in both lanes, positive */
         }
         /* messages: zero for a lane in its first iteration */
         const uint32_t w0 = rec.x & ~fresh;
@@ -132,25 +137,46 @@ struct PairCheck {
         sg = 0;
     }
 
-    /* extrinsic inputs of the owned slots that are (in_pass) or are not
-     * written earlier in the layer, folded into this thread's partial
-     * minimums and sign parity */
-    __device__ __forceinline__ void read(const uint16_t* __restrict__ post, bool in_pass)
+    /* extrinsic input of owned slot k: posterior minus the old message */
+    __device__ __forceinline__ uint32_t extrinsic(const uint16_t* __restrict__ post, int k) const
     {
+        const uint32_t v = sx2(post[addr[k]]);
+        const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(2 * k) * 0x00010001u);
+        const uint32_t sm = lmask(sgn << (15 - 2 * k));
+        return sadd(v, sel(sm, sel(im, n1, n0), sel(im, p1, p0)));
+    }
+
+    __device__ __forceinline__ void fold(uint32_t v)
+    {
+        const uint32_t a = abs2(v);
+        min1 = __vmins2(min1, __vmaxs2(min0, a));
+        min0 = __vmins2(min0, a);
+        sg ^= v;
+    }
+
+    /* every owned slot but the late ones, without branches */
+    __device__ __forceinline__ void read_all(const uint16_t* __restrict__ post)
+    {
+        const uint32_t excl = ~live | inm;
 #pragma unroll
         for (int k = 0; k < S; k++) {
-            if (!((livem >> k) & 1) || (((inm >> k) & 1) != 0) != in_pass)
-                continue;
-            uint32_t v = sx2(post[addr[k]]);
-            const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(2 * k) * 0x00010001u);
-            const uint32_t sm = lmask(sgn << (15 - 2 * k));
-            v = sadd(v, sel(sm, sel(im, n1, n0), sel(im, p1, p0)));
+            uint32_t v = extrinsic(post, k);
+            v = ((excl >> (2 * k)) & 1u) ? 0x00FF00FFu : v;
             x[k] = v;
-            const uint32_t a = abs2(v);
-            min1 = __vmins2(min1, __vmaxs2(min0, a));
-            min0 = __vmins2(min0, a);
-            sg ^= v;
+            fold(v);
         }
+    }
+
+    /* the late slots (their bits were written by earlier levels) */
+    __device__ __forceinline__ void read_late(const uint16_t* __restrict__ post)
+    {
+#pragma unroll
+        for (int k = 0; k < S; k++)
+            if ((inm >> (2 * k)) & 1u) {
+                const uint32_t v = extrinsic(post, k);
+                x[k] = v;
+                fold(v);
+            }
     }
 
     /* combine with the partner thread; offset 1 and the cap at 127 */
@@ -164,38 +190,46 @@ struct PairCheck {
         sg ^= bs;
         mn0 = __viaddmax_s16x2(__vmins2(min0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
         mn1 = __viaddmax_s16x2(__vmins2(min1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
-        min0p1 = __vadd2(min0, 0x00010001u);
     }
 
-    /* new posteriors of the owned slots that are (out_pass) or are not read
-     * by a later check of the layer */
-    __device__ __forceinline__ void write(uint16_t* __restrict__ post, bool out_pass)
+    /* new posterior of owned slot k (two bytes), and its masks: lanes where
+     * |x| is above min0 (the slot does not hold the minimum) and lanes whose
+     * outgoing message is negative */
+    __device__ __forceinline__ uint32_t update(int k, uint32_t& above, uint32_t& neg) const
+    {
+        const uint32_t v = x[k];
+        above = lmask(__viaddmin_s16x2(v, min0, __vsub2(min0, v))); /* min0 - |x| < 0 */
+        neg = lmask(sg ^ v);
+        const uint32_t o = __vsub2(sel(above, mn0, mn1) ^ neg, neg);
+        return pk2(sadd(v, o));
+    }
+
+    /* posteriors that later levels of the layer read */
+    __device__ __forceinline__ void write_early(uint16_t* __restrict__ post) const
     {
 #pragma unroll
-        for (int k = 0; k < S; k++) {
-            if (!((livem >> k) & 1) || (((outm >> k) & 1) != 0) != out_pass)
-                continue;
-            const uint32_t v = x[k];
-            const uint32_t eq = lmask(__vsub2(abs2(v), min0p1)); /* |x| == min0 */
-            const uint32_t sm = lmask(sg ^ v);
-            const uint32_t o = __vsub2(sel(eq, mn1, mn0) ^ sm, sm);
-            post[addr[k]] = (uint16_t)pk2(sadd(v, o));
-        }
+        for (int k = 0; k < S; k++)
+            if ((outm >> (2 * k)) & 1u) {
+                uint32_t above, neg;
+                post[addr[k]] = (uint16_t)update(k, above, neg);
+            }
     }
 
-    /* the node's compressed messages for both lanes, stored by thread 0:
-     * the slot holding min0 and one sign bit per slot */
-    __device__ __forceinline__ void record(unsigned gmask, uint2* __restrict__ dst)
+    /* every other posterior (predicated stores) and the node's compressed
+     * messages for both lanes, stored by thread 0: the slot holding min0 and
+     * one sign bit per slot */
+    __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, unsigned gmask, uint2* __restrict__ dst)
     {
+        const uint32_t wm = live & ~outm;
         uint32_t nidx = 0, nsg = 0; /* nidx per lane: 2k + 1 of an owned slot holding min0, 0 if none */
 #pragma unroll
         for (int k = 0; k < S; k++) {
-            if (r + 2 * k >= D)
-                continue;
-            const uint32_t v = x[k];
-            const uint32_t eq = lmask(__vsub2(abs2(v), min0p1));
-            nidx = sel(eq, (uint32_t)(2 * k + 1) * 0x00010001u, nidx);
-            nsg |= lmask(sg ^ v) & (0x00010001u << (2 * k));
+            uint32_t above, neg;
+            const uint32_t nv = update(k, above, neg);
+            if ((wm >> (2 * k)) & 1u)
+                post[addr[k]] = (uint16_t)nv;
+            nidx = sel(above, nidx, (uint32_t)(2 * k + 1) * 0x00010001u);
+            nsg |= neg & (0x00010001u << (2 * k));
         }
         nsg <<= r; /* bit 2k -> slot 2k + r (slots stay below 16: no carry across lanes) */
         const uint32_t found = lmask(__vsub2(0u, nidx)); /* lanes with nidx > 0 */
@@ -338,7 +372,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
     PairCheck<DM, EXACT> ck;
     if (active) {
         ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, t & 1, rec, fresh, meta);
-        ck.read(fr.post, false);
+        ck.read_all(fr.post);
     }
     if (nlev > 1) {
         const int lev = (int)(meta & 0xFF);
@@ -346,9 +380,10 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             const bool mine = active && lev == l;
             const unsigned gm = __ballot_sync(0xFFFFFFFFu, mine);
             if (mine) {
-                ck.read(fr.post, true);
+                if (l > 0)
+                    ck.read_late(fr.post);
                 ck.finish(gm);
-                ck.write(fr.post, true);
+                ck.write_early(fr.post);
             }
             __syncthreads();
         }
@@ -358,10 +393,8 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             ck.finish(gm);
     }
     const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
-    if (active) {
-        ck.write(fr.post, false);
-        ck.record(gm, msg + kQCp * i + j);
-    }
+    if (active)
+        ck.write_rest(fr.post, gm, msg + kQCp * i + j);
     __syncthreads();
 }
 

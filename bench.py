@@ -124,18 +124,23 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
-def profiled_traffic():
-    """DRAM bytes per decode launch from the committed ncu summary, if any."""
+def profiled_figures():
+    """Figures of the committed ncu summary of the decode kernel: DRAM bytes
+    per full-size launch, issue and ALU-pipe utilisation (percent)."""
     path = os.path.join(ROOT, "profiles", "ldpc_decode_normal_3_5.txt")
+    out = {}
     if not os.path.exists(path):
-        return None
+        return out
+    keys = {"dram_bytes_per_launch_full_size": "traffic", "issue_active_pct": "issue_pct",
+            "alu_pipe_pct": "alu_pct"}
     for line in open(path):
-        if line.startswith("dram_bytes_per_launch_full_size:"):
+        k = line.split(":", 1)[0]
+        if k in keys:
             try:
-                return float(line.split(":", 1)[1].split()[0])
+                out[keys[k]] = float(line.split(":", 1)[1].split()[0])
             except ValueError:
-                return None
-    return None
+                pass
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -332,7 +337,8 @@ def run_b200(args):
     except Exception:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = profiled_traffic()
+    prof = profiled_figures()
+    traffic = prof.get("traffic")
     roofline = {
         "bound": "smem",
         "kernel": kernel_name,
@@ -344,6 +350,10 @@ def run_b200(args):
         "algorithmic_bytes_per_launch": smem_bytes,
         "bytes_per_unit": "4 x E = %d B per frame-iteration (E = %d edges)" % (4 * edges, edges),
         "traffic": traffic,
+        "traffic_note": "DRAM bytes read + written per launch (ncu, small case scaled by frames), "
+                        "against the HBM algorithmic bytes below",
+        "issue": {"issue_active_pct": prof.get("issue_pct"), "alu_pipe_pct": prof.get("alu_pct"),
+                  "note": "ncu on the profiled small case: integer issue on the ALU pipe binds"},
         "hbm": {"achieved": hbm_bytes / kern_s / 1e9, "peak": hbm_peak,
                 "frac": hbm_bytes / kern_s / 1e9 / hbm_peak, "unit": "GB/s",
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",

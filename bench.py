@@ -281,14 +281,16 @@ def run_b200(args):
         l, inf, _ = dec.generate(F, es, seed=1000003 * (rank + 1) + k, constellation=CONST, info=True)
         llr.append(l)
         info.append(inf)
-    out = torch.empty((F, dec.nbytes), dtype=torch.uint8, device="cuda")
+    outs = [torch.empty((F, dec.nbytes), dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
+    out = outs[0]
     iters = [torch.empty(F, dtype=torch.int32, device="cuda") for _ in range(args.steps)]
     oks = [torch.empty(F, dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
     errs = torch.zeros(args.steps, dtype=torch.int64, device="cuda")
     torch.cuda.synchronize()
 
-    def step(k, it_buf, ok_buf):
-        dec.decode_device(llr[k % len(llr)], MAX_ITER, out=out, iters=it_buf, ok=ok_buf)
+    def step(k, it_buf, ok_buf, out_buf=None):
+        dec.decode_device(llr[k % len(llr)], MAX_ITER, out=out if out_buf is None else out_buf, iters=it_buf,
+                          ok=ok_buf)
 
     for k in range(args.warmup):
         step(k, iters[0], oks[0])
@@ -304,11 +306,12 @@ def run_b200(args):
         dist.barrier()
     for k in range(args.steps):
         ev[k][0].record(stream)
-        step(args.warmup + k, iters[k], oks[k])
+        step(args.warmup + k, iters[k], oks[k], outs[k])
         ev[k][1].record(stream)
-        # frame errors of this step (outside the kernel's events)
-        errs[k] = (out != info[(args.warmup + k) % len(info)]).any(dim=1).sum()
     torch.cuda.synchronize()
+    # frame errors of every step, after the timed region
+    for k in range(args.steps):
+        errs[k] = (outs[k] != info[(args.warmup + k) % len(info)]).any(dim=1).sum()
     clocks = sampler.stop()
     launch_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = ev[0][0].elapsed_time(ev[-1][1])
@@ -359,6 +362,7 @@ def run_b200(args):
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_launch": hbm_bytes},
         "avg_launch_ms": statistics.mean(launch_ms),
+        "gap_ms_per_step": (total_ms - sum(launch_ms)) / args.steps,
         "sm_mhz_median": sm_mhz,
     }
 

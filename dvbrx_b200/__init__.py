@@ -101,6 +101,10 @@ def lib():
         L.drx_ldpc_set_variant.restype = ip
         L.drx_ldpc_device_error.argtypes = [vp]
         L.drx_ldpc_device_error.restype = ip
+        L.drx_ldpc_set_learned.argtypes = [vp, ip, ip, vp, vp, vp]
+        L.drx_ldpc_set_learned.restype = ip
+        L.drx_ldpc_decode_learned_device.argtypes = [vp, vp, sz, vp, sz, vp, vp, vp, ip, ip, ip, vp]
+        L.drx_ldpc_decode_learned_device.restype = ip
         _lib = L
     return _lib
 
@@ -249,6 +253,50 @@ class Ldpc:
 
     def device_error(self):
         return self._lib.drx_ldpc_device_error(self.h)
+
+    def set_learned(self, scale, offset, class_of_degree):
+        """``drx_ldpc_set_learned``: scale and offset tables [iters, nclass]
+        (anything numpy converts to float32) and the class of every check
+        degree (int8[33]); ``None`` removes the table."""
+        if scale is None:
+            if self._lib.drx_ldpc_set_learned(self.h, 0, 0, None, None, None) != 0:
+                raise RuntimeError("drx_ldpc_set_learned: " + last_error())
+            return
+        b = np.ascontiguousarray(np.asarray(scale, dtype=np.float32))
+        a = np.ascontiguousarray(np.asarray(offset, dtype=np.float32))
+        cod = np.ascontiguousarray(np.asarray(class_of_degree, dtype=np.int8))
+        assert b.shape == a.shape and b.ndim == 2 and cod.size == 33
+        r = self._lib.drx_ldpc_set_learned(self.h, b.shape[0], b.shape[1], cod.ctypes.data, b.ctypes.data,
+                                          a.ctypes.data)
+        if r != 0:
+            raise RuntimeError("drx_ldpc_set_learned: " + last_error())
+
+    def decode_learned(self, llr, learned_iters, plain_max_iter=0, out=None, iters=None, ok=None,
+                       fallback=None, stream=None):
+        """``drx_ldpc_decode_learned_device`` on torch CUDA tensors: the
+        learned decode (at most learned_iters iterations), then, with
+        plain_max_iter > 0, the plain decoder on the frames whose syndrome
+        still fails.  Returns (bits, iterations, ok, fallback)."""
+        import torch
+
+        assert llr.is_cuda and llr.dtype == torch.int8 and llr.dim() == 2 and llr.stride(1) == 1
+        n = llr.shape[0]
+        dev = llr.device
+        if out is None:
+            out = torch.empty((n, self.nbytes), dtype=torch.uint8, device=dev)
+        if iters is None:
+            iters = torch.empty(n, dtype=torch.int32, device=dev)
+        if ok is None:
+            ok = torch.empty(n, dtype=torch.uint8, device=dev)
+        if fallback is None:
+            fallback = torch.empty(n, dtype=torch.uint8, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        r = self._lib.drx_ldpc_decode_learned_device(
+            self.h, llr.data_ptr(), llr.stride(0), out.data_ptr(), out.stride(0), iters.data_ptr(),
+            ok.data_ptr(), fallback.data_ptr(), n, int(learned_iters), int(plain_max_iter), stream_handle(s))
+        if r != 0:
+            raise RuntimeError("drx_ldpc_decode_learned_device: " + last_error())
+        return out, iters, ok, fallback
 
 
 TILING_ONE_LAUNCH, TILING_PER_CODE = 1, 2  # DRX_TILING_*

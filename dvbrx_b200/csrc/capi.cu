@@ -187,9 +187,20 @@ bool upload_code(drx_ldpc* d)
     return true;
 }
 
+/* Per-frame extras of a launch: learned check nodes, a row list and a
+ * frame count read on the device (nframes is then an upper bound). */
+struct Extra {
+    const uint32_t* learn = nullptr;
+    const int8_t* learn_class = nullptr;
+    int learn_iters = 0;
+    const int32_t* rows = nullptr;
+    const int* nframes_dev = nullptr;
+};
+
 /* Queue one decode of nframes device-resident frames. */
 int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, size_t out_stride,
-            int32_t* iters, uint8_t* ok, int nframes, int max_iter, int stop, cudaStream_t s)
+            int32_t* iters, uint8_t* ok, int nframes, int max_iter, int stop, cudaStream_t s,
+            const Extra* x = nullptr)
 {
     if (nframes <= 0)
         return 0;
@@ -219,6 +230,17 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
     p.nframes = nframes;
     p.max_iter = max_iter;
     p.err = d->err;
+    if (x) {
+        if (stop != 0) {
+            set_err("learned check nodes and row lists need per-frame stopping");
+            return -1;
+        }
+        p.learn = x->learn;
+        p.learn_class = x->learn_class;
+        p.learn_iters = x->learn_iters;
+        p.rows = x->rows;
+        p.nframes_dev = x->nframes_dev;
+    }
     int grid;
     if (stop == 0 && use_pair(d)) {
         /* two frames per CTA */
@@ -264,6 +286,37 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
     p.msg = d->msg;
     p.msg_stride = decode_msg_bytes(d->code.R, d->code.dclass);
     return cuda_ok(launch_decode(p, d->code.dclass, d->smem, grid, s), "decoder launch") ? 0 : -1;
+}
+
+/* Rows whose learned decode failed: appended to rows (count in *count,
+ * zeroed by the caller), flagged in fallback (may be null). */
+__global__ void k_fallback_rows(const uint8_t* __restrict__ ok, int n, int32_t* __restrict__ rows, int* count,
+                                uint8_t* __restrict__ fallback)
+{
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n; f += gridDim.x * blockDim.x) {
+        const bool fail = ok[f] == 0;
+        if (fallback)
+            fallback[f] = fail ? 1 : 0;
+        if (fail)
+            rows[atomicAdd(count, 1)] = f;
+    }
+}
+
+bool ensure_fallback(drx_ldpc* d, size_t nframes)
+{
+    if (d->fb_cap >= nframes)
+        return true;
+    cudaStreamSynchronize(d->stream);
+    cudaFree(d->fb_rows);
+    cudaFree(d->fb_ok);
+    d->fb_rows = nullptr;
+    d->fb_ok = nullptr;
+    d->fb_cap = 0;
+    if (!cuda_ok(cudaMalloc(&d->fb_rows, nframes * sizeof(int32_t) + 16), "cudaMalloc(fallback rows)") ||
+        !cuda_ok(cudaMalloc(&d->fb_ok, nframes), "cudaMalloc(fallback flags)"))
+        return false;
+    d->fb_cap = nframes;
+    return true;
 }
 
 }  // namespace
@@ -349,6 +402,9 @@ void drx_ldpc_free(drx_ldpc* d)
         cudaStreamSynchronize(d->stream);
     release_stage(d);
     cudaFree(d->msg);
+    cudaFree(d->fb_rows);
+    cudaFree(d->fb_ok);
+    cudaFree(d->learn);
     cudaFree(d->sync);
     cudaFree(d->work);
     cudaFree(d->err);
@@ -437,6 +493,97 @@ int drx_ldpc_decode_device(drx_ldpc* d, const int8_t* llr, size_t llr_stride, ui
     }
     return enqueue(d, llr, llr_stride, out, out_stride, iters, ok, nframes, max_iter, stop,
                    stream ? (cudaStream_t)stream : d->stream);
+}
+
+int drx_ldpc_set_learned(drx_ldpc* d, int iters, int nclass, const int8_t* class_of_degree,
+                         const float* scale, const float* offset)
+{
+    if (!d) {
+        set_err("NULL handle");
+        return -1;
+    }
+    if (iters == 0) {
+        d->learn_iters = 0;
+        return 0;
+    }
+    if (iters < 0 || iters > kLearnMaxIters || nclass < 1 || nclass > kLearnClasses || !class_of_degree ||
+        !scale || !offset) {
+        set_err("learned table: 1..32 iterations, 1..8 classes and all arrays are required");
+        return -1;
+    }
+    for (int k = 0; k <= 32; k++)
+        if (class_of_degree[k] < 0 || class_of_degree[k] >= nclass) {
+            set_err("learned table: class of a degree out of range");
+            return -1;
+        }
+    std::vector<uint32_t> tab((size_t)iters * kLearnClasses, 0);
+    for (int t = 0; t < iters; t++)
+        for (int k = 0; k < nclass; k++) {
+            const float b = scale[t * nclass + k], a = offset[t * nclass + k];
+            if (!(b == b) || !(a == a)) {
+                set_err("learned table: NaN parameter");
+                return -1;
+            }
+            const long bq = std::min(std::max(lrintf(b * 256.0f), 0L), 65535L);
+            const long aq = std::min(std::max(lrintf(a * 256.0f), -32768L), 32767L);
+            tab[(size_t)t * kLearnClasses + k] = (uint32_t)bq | (uint32_t)(uint16_t)(int16_t)aq << 16;
+        }
+    if (!d->learn) {
+        if (!cuda_ok(cudaMalloc(&d->learn, sizeof(uint32_t) * kLearnMaxIters * kLearnClasses + 64),
+                     "cudaMalloc(learned table)"))
+            return -1;
+    }
+    cudaStreamSynchronize(d->stream);
+    if (!cuda_ok(cudaMemcpy(d->learn, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice),
+                 "cudaMemcpy(learned table)") ||
+        !cuda_ok(cudaMemcpy((char*)d->learn + sizeof(uint32_t) * kLearnMaxIters * kLearnClasses,
+                            class_of_degree, 33, cudaMemcpyHostToDevice),
+                 "cudaMemcpy(learned classes)"))
+        return -1;
+    d->learn_iters = iters;
+    return 0;
+}
+
+int drx_ldpc_decode_learned_device(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out,
+                                   size_t out_stride, int32_t* iters, uint8_t* ok, uint8_t* fallback,
+                                   int nframes, int learned_iters, int plain_max_iter, void* stream)
+{
+    if (!d || (nframes > 0 && (!llr || !out))) {
+        set_err("NULL argument");
+        return -1;
+    }
+    if (d->learn_iters <= 0) {
+        set_err("no learned table on this handle (drx_ldpc_set_learned)");
+        return -1;
+    }
+    if (nframes <= 0)
+        return 0;
+    cudaStream_t s = stream ? (cudaStream_t)stream : d->stream;
+    if (!ensure_fallback(d, (size_t)nframes))
+        return -1;
+    uint8_t* okb = ok ? ok : d->fb_ok;
+    Extra x;
+    x.learn = d->learn;
+    x.learn_class = (const int8_t*)((const char*)d->learn + sizeof(uint32_t) * kLearnMaxIters * kLearnClasses);
+    x.learn_iters = d->learn_iters;
+    if (enqueue(d, llr, llr_stride, out, out_stride, iters, okb, nframes, learned_iters, 0, s, &x))
+        return -1;
+    if (plain_max_iter <= 0) {
+        if (fallback && !cuda_ok(cudaMemsetAsync(fallback, 0, (size_t)nframes, s), "cudaMemsetAsync"))
+            return -1;
+        return 0;
+    }
+    int* count = (int*)(d->fb_rows + d->fb_cap);
+    if (!cuda_ok(cudaMemsetAsync(count, 0, sizeof(int), s), "cudaMemsetAsync"))
+        return -1;
+    const int blocks = std::min((nframes + 255) / 256, 4 * d->sms);
+    k_fallback_rows<<<blocks, 256, 0, s>>>(okb, nframes, d->fb_rows, count, fallback);
+    if (!cuda_ok(cudaGetLastError(), "fallback rows"))
+        return -1;
+    Extra y;
+    y.rows = d->fb_rows;
+    y.nframes_dev = count;
+    return enqueue(d, llr, llr_stride, out, out_stride, iters, okb, nframes, plain_max_iter, 0, s, &y);
 }
 
 int drx_ldpc_decode_host(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t* iters,

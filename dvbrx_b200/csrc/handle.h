@@ -36,6 +36,15 @@ struct drx_ldpc {
     unsigned* sync = nullptr;
     size_t sync_cap = 0;
     int* err = nullptr;
+    /* learned check nodes: kLearnMaxIters rows of kLearnClasses words, then
+     * the 33 degree classes; learn_iters rows in use (0: none) */
+    uint32_t* learn = nullptr;
+    int learn_iters = 0;
+    /* fallback of the learned decode: failing rows (fb_cap + a count word)
+     * and flags when the caller passes none */
+    int32_t* fb_rows = nullptr;
+    uint8_t* fb_ok = nullptr;
+    size_t fb_cap = 0;
     /* staging of the host-pointer calls */
     int8_t* h_llr = nullptr;
     uint8_t* h_out = nullptr;

@@ -79,7 +79,8 @@ __device__ __forceinline__ int sat8(int v) { return max(-128, min(127, v)); }
 template <int CNT, int IDXMASK>
 __device__ __forceinline__ void check_node_n(int8_t* __restrict__ post, const int2* __restrict__ ent,
                                              int K, int q, int i, int j, bool first, uint32_t meta,
-                                             uint32_t sgn, uint32_t& meta_out, uint32_t& sgn_out)
+                                             uint32_t sgn, bool learned, uint32_t lw, uint32_t& meta_out,
+                                             uint32_t& sgn_out)
 {
     constexpr int D = CNT + 2;
     int addr[D];
@@ -118,7 +119,8 @@ __device__ __forceinline__ void check_node_n(int8_t* __restrict__ post, const in
         min0 = min(min0, a);
         sg ^= v;
     }
-    const int mn0 = max(min(min0, 127) - 1, 0), mn1 = max(min(min1, 127) - 1, 0);
+    const int mn0 = learned ? learned_mag(min(min0, 127), lw) : max(min(min0, 127) - 1, 0);
+    const int mn1 = learned ? learned_mag(min(min1, 127), lw) : max(min(min1, 127) - 1, 0);
     int nidx = 0;
     uint32_t nsg = 0;
 #pragma unroll
@@ -142,15 +144,15 @@ __device__ __forceinline__ void check_node_n(int8_t* __restrict__ post, const in
 template <int DMAX>
 __device__ __forceinline__ void check_node(int8_t* __restrict__ post, const int2* __restrict__ ent,
                                            int cnt, int K, int q, int i, int j, bool first,
-                                           uint32_t meta, uint32_t sgn, uint32_t& meta_out,
-                                           uint32_t& sgn_out)
+                                           uint32_t meta, uint32_t sgn, bool learned, uint32_t lw,
+                                           uint32_t& meta_out, uint32_t& sgn_out)
 {
     constexpr int M = DMAX > 16 ? 31 : 15;
 #define DRXG_CASE(n)                                                                           \
     case n:                                                                                    \
         if (n + 2 <= DMAX)                                                                     \
             check_node_n<(n + 2 <= DMAX ? n : 1), M>(post, ent, K, q, i, j, first, meta, sgn, \
-                                                     meta_out, sgn_out);                       \
+                                                     learned, lw, meta_out, sgn_out);          \
         break;
     switch (cnt) {
         DRXG_CASE(1) DRXG_CASE(2) DRXG_CASE(3) DRXG_CASE(4) DRXG_CASE(5) DRXG_CASE(6)
@@ -259,9 +261,9 @@ __device__ bool syndrome_fails(const DevCode& c, const Frame& fr, volatile int* 
 }
 
 /* One decoding iteration: every step (layer level) in order. */
-template <int DMAX>
+template <int DMAX, bool LEARNED>
 __device__ void iterate(const DevCode& c, const Frame& fr, typename MsgWord<DMAX>::T* __restrict__ msg,
-                        bool first)
+                        bool first, int lrow)
 {
     typedef typename MsgWord<DMAX>::T W;
     const int t = threadIdx.x;
@@ -290,8 +292,11 @@ __device__ void iterate(const DevCode& c, const Frame& fr, typename MsgWord<DMAX
             if (!first)
                 unpack(w, meta, sgn);
             const int e0 = fr.eoff[i];
-            check_node<DMAX>(fr.post, fr.ent + e0, fr.eoff[i + 1] - e0, c.K, c.q, i, j, first, meta,
-                             sgn, mo, so);
+            const int cnt = fr.eoff[i + 1] - e0;
+            uint32_t lw = 0;
+            if (LEARNED)
+                lw = s_learn_tab[lrow + s_learn_cls[cnt + 2 - ((i | j) == 0)]];
+            check_node<DMAX>(fr.post, fr.ent + e0, cnt, c.K, c.q, i, j, first, meta, sgn, LEARNED, lw, mo, so);
             W wo;
             pack(wo, mo, so);
             st_msg(msg + kQC * i + start + t, wo);
@@ -349,10 +354,10 @@ __device__ int team_vote(unsigned* slot, int G, bool fail, int* err)
 }
 
 template <int DMAX>
-__device__ void decode_frame(const DevCode& c, const Frame& fr, const DecodeParams& p, int f,
-                             typename MsgWord<DMAX>::T* msg, volatile int* sflag, unsigned* sync)
+__device__ __forceinline__ void decode_frame(const DevCode& c, const Frame& fr, const DecodeParams& p, int nframes, int f,
+                             typename MsgWord<DMAX>::T* msg, volatile int* sflag, unsigned* sync, int lT)
 {
-    const bool real = f < p.nframes;
+    const bool real = f < nframes;
     const int row = real && p.rows ? p.rows[f] : f;
     if (real)
         load_frame(c, fr, p.llr + (size_t)row * p.llr_stride);
@@ -375,8 +380,12 @@ __device__ void decode_frame(const DevCode& c, const Frame& fr, const DecodePara
         }
         if (ok || it >= p.max_iter)
             break;
-        if (real)
-            iterate<DMAX>(c, fr, msg, it == 0);
+        if (real) {
+            if (lT)
+                iterate<DMAX, true>(c, fr, msg, it == 0, learn_row(it, lT));
+            else
+                iterate<DMAX, false>(c, fr, msg, it == 0, 0);
+        }
         it++;
     }
     if (real) {
@@ -399,6 +408,8 @@ __global__ void __launch_bounds__(kThreads, MINB) k_decode(DecodeParams p)
     __shared__ int s_flag;
     const DevCode c = *p.code;
     const Frame fr = stage_code(c, smem);
+    const int lT = stage_learn(p.learn, p.learn_class, p.learn_iters);
+    const int nframes = p.nframes_dev ? *p.nframes_dev : p.nframes;
     typedef typename MsgWord<DMAX>::T W;
     W* msg = (W*)((char*)p.msg + (size_t)blockIdx.x * p.msg_stride);
     if (threadIdx.x == 0)
@@ -411,9 +422,9 @@ __global__ void __launch_bounds__(kThreads, MINB) k_decode(DecodeParams p)
             __syncthreads();
             const int f = s_frame;
             __syncthreads();
-            if (f >= p.nframes)
+            if (f >= nframes)
                 break;
-            decode_frame<DMAX>(c, fr, p, f, msg, &s_flag, nullptr);
+            decode_frame<DMAX>(c, fr, p, nframes, f, msg, &s_flag, nullptr, lT);
         }
     } else {
         const int G = p.group;
@@ -422,7 +433,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_decode(DecodeParams p)
         const int per = p.max_iter + 1;
         for (int g = team, k = 0; g < ngroups; g += p.nteams, k++) {
             unsigned* sync = p.team_sync + 2 * (size_t)per * ((size_t)team * ((ngroups + p.nteams - 1) / p.nteams) + k);
-            decode_frame<DMAX>(c, fr, p, g * G + member, msg, &s_flag, sync);
+            decode_frame<DMAX>(c, fr, p, nframes, g * G + member, msg, &s_flag, sync, lT);
         }
     }
 }
@@ -453,6 +464,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_decode_mix(MixParams mp)
     int staged = -1;
     DevCode c{};
     Frame fr{};
+    int lT = 0;
     for (;;) {
         if (threadIdx.x == 0)
             s_k = (int)atomicAdd(mp.work, 1u);
@@ -465,10 +477,11 @@ __global__ void __launch_bounds__(kThreads, MINB) k_decode_mix(MixParams mp)
         if (ci != staged) {
             c = *mp.codes[ci];
             fr = stage_code(c, smem);
+            lT = mp.learn ? stage_learn(mp.learn[ci], mp.learn_class[ci], mp.learn_iters[ci]) : 0;
             staged = ci;
             __syncthreads();
         }
-        decode_frame<DMAX>(c, fr, p, k, msg, &s_flag, nullptr);
+        decode_frame<DMAX>(c, fr, p, mp.nframes, k, msg, &s_flag, nullptr, lT);
     }
 }
 

@@ -45,7 +45,52 @@ struct DecodeParams {
     int* err;              /* device error word (0 = fine) */
     const int32_t* rows;   /* per-frame mode, optional: work item k is row rows[k] of
                               llr / out / iters / ok (null: row k) */
+    const int* nframes_dev; /* per-frame mode, optional: the number of work items, read on
+                               the device at kernel start (replaces nframes) */
+    const uint32_t* learn; /* learned check nodes (null: the plain offset 1): learn_iters
+                              rows of kLearnClasses words, see learned_mag */
+    const int8_t* learn_class; /* degree class of every check degree 0..32 */
+    int learn_iters;
 };
+
+/* Learned check nodes (the neural offset / scaled min-sum at int8): the
+ * outgoing magnitude of a node in iteration t is
+ *     max((scale * m - offset + 128) >> 8, 0),   m = min(minimum, 127),
+ * with scale and offset in Q8 from row min(t, learn_iters - 1) and the
+ * check's degree class: word = scale (16 bits) | offset (signed 16) << 16.
+ * Scale 256 and offset 256 give max(m - 1, 0), the plain decoder. */
+constexpr int kLearnClasses = 8;
+constexpr int kLearnMaxIters = 32;
+#ifdef __CUDACC__
+__device__ __forceinline__ int learned_mag(int m, uint32_t w)
+{
+    return max(((int)(w & 0xFFFFu) * m - ((int)w >> 16) + 128) >> 8, 0);
+}
+
+/* The learned table of a launch, staged in shared memory by stage_learn
+ * (one copy per translation unit; kernels that never stage it do not
+ * allocate it). */
+static __shared__ uint32_t s_learn_tab[kLearnMaxIters * kLearnClasses];
+static __shared__ int8_t s_learn_cls[33];
+
+/* Stage a learned table (T rows of kLearnClasses words, classes of the
+ * degrees 0..32); returns the staged row count, 0 for the plain decoder.
+ * The caller synchronises the block before the table is read. */
+__device__ __forceinline__ int stage_learn(const uint32_t* tab, const int8_t* cls, int T)
+{
+    if (!tab || !cls || T <= 0)
+        return 0;
+    T = min(T, kLearnMaxIters);
+    for (int k = threadIdx.x; k < T * kLearnClasses; k += blockDim.x)
+        s_learn_tab[k] = tab[k];
+    for (int k = threadIdx.x; k < 33; k += blockDim.x)
+        s_learn_cls[k] = cls[k];
+    return T;
+}
+
+/* First word of the learned row of iteration `it` (T > 0). */
+__device__ __forceinline__ int learn_row(int it, int T) { return kLearnClasses * min(it, T - 1); }
+#endif
 
 /* A batch of frames of several codes (one launch over all of them). */
 struct MixParams {
@@ -63,6 +108,11 @@ struct MixParams {
     unsigned* work;
     void* msg;
     size_t msg_stride;
+    /* learned check nodes per code index (null entries, or a null array:
+     * the plain offset 1); layout as DecodeParams::learn */
+    const uint32_t* const* learn;
+    const int8_t* const* learn_class;
+    const int* learn_iters;
 };
 
 /* One persistent launch over a mixed batch: one frame per CTA, the CTA

@@ -179,8 +179,9 @@ struct PairCheck {
             }
     }
 
-    /* combine with the partner thread; offset 1 and the cap at 127 */
-    __device__ __forceinline__ void finish(unsigned gmask)
+    /* combine with the partner thread; the cap at 127 and offset 1, or the
+     * learned scale and offset of each lane's iteration (lpA, lpB) */
+    __device__ __forceinline__ void finish(unsigned gmask, bool learned, uint32_t lpA, uint32_t lpB)
     {
         const uint32_t b0 = __shfl_xor_sync(gmask, min0, 1);
         const uint32_t b1 = __shfl_xor_sync(gmask, min1, 1);
@@ -188,8 +189,14 @@ struct PairCheck {
         min1 = __vmins2(__vmaxs2(min0, b0), __vmins2(min1, b1));
         min0 = __vmins2(min0, b0);
         sg ^= bs;
-        mn0 = __viaddmax_s16x2(__vmins2(min0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
-        mn1 = __viaddmax_s16x2(__vmins2(min1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+        if (learned) {
+            const uint32_t c0 = __vmins2(min0, 0x007F007Fu), c1 = __vmins2(min1, 0x007F007Fu);
+            mn0 = (uint32_t)learned_mag(c0 & 0xFFFF, lpA) | (uint32_t)learned_mag(c0 >> 16, lpB) << 16;
+            mn1 = (uint32_t)learned_mag(c1 & 0xFFFF, lpA) | (uint32_t)learned_mag(c1 >> 16, lpB) << 16;
+        } else {
+            mn0 = __viaddmax_s16x2(__vmins2(min0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+            mn1 = __viaddmax_s16x2(__vmins2(min1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+        }
     }
 
     /* new posterior of owned slot k (two bytes), and its masks: lanes where
@@ -364,11 +371,21 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
  */
 template <int DM, bool EXACT>
 __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev, uint2 rec,
-                                           unsigned long long meta, uint32_t fresh, uint2* __restrict__ msg)
+                                           unsigned long long meta, uint32_t fresh, uint2* __restrict__ msg,
+                                           int lA, int lB)
 {
     const int t = threadIdx.x;
     const bool active = t < 2 * kQCp;
     const int j = t >> 1;
+    /* learned scale / offset words of the check for both lanes */
+    auto lwords = [&](uint32_t& a, uint32_t& b) {
+        a = b = 0;
+        if (lA >= 0) {
+            const int k = s_learn_cls[(EXACT ? DM : cnt + 2) - ((i | j) == 0)];
+            a = s_learn_tab[lA + k];
+            b = s_learn_tab[lB + k];
+        }
+    };
     PairCheck<DM, EXACT> ck;
     if (active) {
         ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, t & 1, rec, fresh, meta);
@@ -382,15 +399,20 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             if (mine) {
                 if (l > 0)
                     ck.read_late(fr.post);
-                ck.finish(gm);
+                uint32_t wa, wb;
+                lwords(wa, wb);
+                ck.finish(gm, lA >= 0, wa, wb);
                 ck.write_early(fr.post);
             }
             __syncthreads();
         }
     } else {
         const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
-        if (active)
-            ck.finish(gm);
+        if (active) {
+            uint32_t wa, wb;
+            lwords(wa, wb);
+            ck.finish(gm, lA >= 0, wa, wb);
+        }
     }
     const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
     if (active)
@@ -403,7 +425,8 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
  * the two information-link counts A <= B of its codes (exact-degree check
  * nodes), or, with GDM > 0, for any count up to GDM - 2 (predicated). */
 template <int A, int B, int GDM>
-__device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __restrict__ msg, uint32_t fresh)
+__device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __restrict__ msg, uint32_t fresh,
+                             int lA, int lB)
 {
     const int t = threadIdx.x;
     const int j = t >> 1;
@@ -424,11 +447,11 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __res
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
         const int nlev = c.nlev[i];
         if (GDM > 0)
-            layer_pair<(GDM > 0 ? GDM : 2), false>(fr, c, i, cnt, nlev, rec, meta, fresh, msg);
+            layer_pair<(GDM > 0 ? GDM : 2), false>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else if (A == B || cnt == A)
-            layer_pair<A + 2, true>(fr, c, i, cnt, nlev, rec, meta, fresh, msg);
+            layer_pair<A + 2, true>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else
-            layer_pair<B + 2, true>(fr, c, i, cnt, nlev, rec, meta, fresh, msg);
+            layer_pair<B + 2, true>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
     }
 }
 
@@ -454,6 +477,8 @@ __global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
     __shared__ int s_frame[2], s_iter[2], s_flag, s_reload;
     const DevCode c = *p.code;
     const PairFrame fr = stage_pair(c, smem);
+    const int lT = stage_learn(p.learn, p.learn_class, p.learn_iters);
+    const int nframes = p.nframes_dev ? *p.nframes_dev : p.nframes;
     uint2* msg = (uint2*)((char*)p.msg + (size_t)blockIdx.x * p.msg_stride);
     const int t = threadIdx.x;
     if (t == 0) {
@@ -471,7 +496,7 @@ __global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
                 for (int h = 0; h < 2; h++)
                     if (reload & (1 << h)) {
                         const int f = (int)atomicAdd(p.work, 1u);
-                        s_frame[h] = f < p.nframes ? f : -1;
+                        s_frame[h] = f < nframes ? f : -1;
                         s_iter[h] = 0;
                     }
             }
@@ -514,7 +539,8 @@ __global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
         __syncthreads();
         if (done)
             continue; /* reload, then check the new frames first */
-        iterate_pair<A, B, GDM>(c, fr, msg, fresh);
+        iterate_pair<A, B, GDM>(c, fr, msg, fresh, lT ? learn_row(s_iter[0], lT) : -1,
+                                lT ? learn_row(s_iter[1], lT) : -1);
         fresh = 0;
         if (t == 0) {
             s_iter[0]++;

@@ -212,6 +212,36 @@ int drx_learned_backward(drx_ldpc* d, int nframes, const void* llr_f16, size_t l
                          const int8_t* class_of_degree, float loss_scale, float* dbeta, float* dalpha,
                          float* loss_scratch, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- learned min-sum: int8 inference --------------------------------------
+ *
+ * No counterpart in the reference (its decoder has only the offset 1).
+ * The trained scale and offset tables (iters x nclass floats, row t for
+ * iteration t, as trained with drx_learned_*) are rounded to Q8 and the int8
+ * decoders use, for a node of degree class k in iteration t (rows past the
+ * last repeat it),
+ *     mag = max((scale_q * m - offset_q + 128) >> 8, 0),  m = min(minimum, 127),
+ * with scale_q = round(256 scale) in [0, 65535] and offset_q =
+ * round(256 offset) in [-32768, 32767]; messages and posteriors stay int8
+ * exactly as in the plain decoder.  Scale 1 and offset 1 give the plain
+ * decoder bit for bit.  iters = 0 removes the table.  1 <= iters <= 32,
+ * 1 <= nclass <= 8.  Synchronous; returns 0 or -1. */
+int drx_ldpc_set_learned(drx_ldpc* d, int iters, int nclass, const int8_t* class_of_degree,
+                         const float* scale, const float* offset);
+
+/* The learned decode with the plain decoder as fallback, on device-resident
+ * frames (arguments as drx_ldpc_decode_device, per-frame stopping): every
+ * frame is decoded with the handle's learned table for at most
+ * learned_iters iterations; with plain_max_iter > 0, the frames whose
+ * syndrome still fails are decoded again from their LLRs by the plain
+ * decoder (at most plain_max_iter iterations) and their bits, iterations
+ * and flags replace the learned ones.  fallback (nframes bytes, or NULL)
+ * receives 1 for the re-decoded frames.  The failing rows are gathered on
+ * the device, so the call never waits for the GPU.  Returns 0 if the work
+ * was queued. */
+int drx_ldpc_decode_learned_device(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out,
+                                   size_t out_stride, int32_t* iters, uint8_t* ok, uint8_t* fallback,
+                                   int nframes, int learned_iters, int plain_max_iter, void* stream);
+
 /* The decoding schedule of a code, computed on the host: the number of
  * steps and the largest check degree; for every check (layer-order index
  * 360 i + j) its step (check_step[R]) and its links (links[R][deg_max]:

@@ -82,6 +82,8 @@ def load_orc():
         lib.orc_decode_frame.argtypes = [vp, vp, vp, ip, ctypes.POINTER(ctypes.c_int)]
         lib.orc_decode_frames.argtypes = [vp, vp, vp, vp, vp, ip, ip]
         lib.orc_encode.argtypes = [vp, vp, vp]
+        lib.orc_decode_frame_learned.argtypes = [vp, vp, vp, ip, vp, vp, ip, vp]
+        lib.orc_decode_frame_learned.restype = ip
         _orc = lib
     return _orc
 
@@ -142,6 +144,20 @@ def _ptr_array(rows):
     return arr
 
 
+def learned_words(scale, offset):
+    """Learned tables [iters, nclass] as the decoder's Q8 words
+    [iters, 8]: round-half-even(256 scale) clamped to [0, 65535] in the low
+    half, round-half-even(256 offset) clamped to [-32768, 32767] in the high
+    half."""
+    b = np.asarray(scale, dtype=np.float32)
+    a = np.asarray(offset, dtype=np.float32)
+    bq = np.clip(np.rint(b * np.float32(256)), 0, 65535).astype(np.int64)
+    aq = np.clip(np.rint(a * np.float32(256)), -32768, 32767).astype(np.int64)
+    w = np.zeros((b.shape[0], 8), np.uint32)
+    w[:, : b.shape[1]] = (bq | ((aq & 0xFFFF) << 16)).astype(np.uint32)
+    return np.ascontiguousarray(w)
+
+
 class OrcCode:
     """The restatement for one code."""
 
@@ -182,6 +198,25 @@ class OrcCode:
         ok = np.zeros(n, np.uint8)
         self.lib.orc_decode_frames(self.h, llr.ctypes.data, out.ctypes.data, it.ctypes.data,
                                    ok.ctypes.data, n, max_iter)
+        return out, it, ok
+
+    def decode_frames_learned(self, llr, max_iter, scale, offset, class_of_degree):
+        """This project's learned decoder at int8 (each frame on its own):
+        the scale / offset tables [iters, nclass] are rounded to Q8 as the
+        library does.  Hard bits, iterations, syndrome flags."""
+        words = learned_words(scale, offset)
+        cls = np.ascontiguousarray(np.asarray(class_of_degree, dtype=np.int8))
+        llr = np.ascontiguousarray(llr, dtype=np.int8)
+        n = llr.shape[0]
+        out = np.zeros((n, self.nbytes), np.uint8)
+        it = np.zeros(n, np.int32)
+        ok = np.zeros(n, np.uint8)
+        for f in range(n):
+            itf = ctypes.c_int()
+            ok[f] = self.lib.orc_decode_frame_learned(self.h, llr[f].ctypes.data, out[f].ctypes.data, max_iter,
+                                                      ctypes.byref(itf), words.ctypes.data, words.shape[0],
+                                                      cls.ctypes.data)
+            it[f] = itf.value
         return out, it, ok
 
     def decode_group(self, llr, max_iter):

@@ -169,7 +169,15 @@ static int bad(const orc_code* d, const int8_t* data, const int8_t* pty)
  * parity node), bl its messages.  The compressed variant (ldpc.c:386-462)
  * stores the same clamped messages in another layout, so one restatement
  * serves both. */
-static void check_node(int8_t* const* v, int8_t* bl, int deg, int first)
+/* Learned magnitude of this project's learned decoder (not in the
+ * reference): word = scale_q | offset_q << 16 (Q8), m capped at 127. */
+static inline int learned_mag(int m, uint32_t w)
+{
+    const int r = ((int)(w & 0xFFFFu) * m - ((int32_t)w >> 16) + 128) >> 8;
+    return r > 0 ? r : 0;
+}
+
+static void check_node(int8_t* const* v, int8_t* bl, int deg, int first, const uint32_t* lw)
 {
     int x[MAX_DEG];
     int min0 = 255, min1 = 255, signs = 0;
@@ -182,8 +190,12 @@ static void check_node(int8_t* const* v, int8_t* bl, int deg, int first)
         signs ^= x[c];
     }
     /* offset 1 and the cap at 127 once per node (ldpc.c:350-353) */
-    const int mn0 = (min0 < 127 ? min0 : 127) - 1 > 0 ? (min0 < 127 ? min0 : 127) - 1 : 0;
-    const int mn1 = (min1 < 127 ? min1 : 127) - 1 > 0 ? (min1 < 127 ? min1 : 127) - 1 : 0;
+    int mn0 = (min0 < 127 ? min0 : 127) - 1 > 0 ? (min0 < 127 ? min0 : 127) - 1 : 0;
+    int mn1 = (min1 < 127 ? min1 : 127) - 1 > 0 ? (min1 < 127 ? min1 : 127) - 1 : 0;
+    if (lw) { /* the learned rule replaces offset 1 (scale_q >= 0: mn1 >= mn0 still) */
+        mn0 = learned_mag(min0 < 127 ? min0 : 127, *lw);
+        mn1 = learned_mag(min1 < 127 ? min1 : 127, *lw);
+    }
     for (int c = 0; c < deg; c++) {
         const int a = x[c] < 0 ? -x[c] : x[c];
         const int mag = a == min0 ? (mn0 > mn1 ? mn0 : mn1) : mn0;
@@ -210,8 +222,9 @@ static void lane_load(const orc_code* d, lane* l, const int8_t* llr)
             l->pty[M * i + j] = l->data[d->K + d->q * j + i];
 }
 
-/* ldpc.c:465-517: layers in order, checks j = 0..359 in order. */
-static void update(const orc_code* d, lane* l, int first)
+/* ldpc.c:465-517: layers in order, checks j = 0..359 in order.  lrow /
+ * lcls: a learned table row and the class of each degree, or NULL. */
+static void update(const orc_code* d, lane* l, int first, const uint32_t* lrow, const int8_t* lcls)
 {
     int8_t* v[MAX_DEG];
     for (int i = 0; i < d->q; i++) {
@@ -226,7 +239,7 @@ static void update(const orc_code* d, lane* l, int first)
             int deg = cnt + 1;
             if (pp >= 0)
                 v[deg++] = l->pty + pp;
-            check_node(v, l->bl + (size_t)(d->CNL + 2) * cn, deg, first);
+            check_node(v, l->bl + (size_t)(d->CNL + 2) * cn, deg, first, lrow ? lrow + lcls[deg] : NULL);
         }
     }
 }
@@ -281,7 +294,7 @@ int orc_decode_group(const orc_code* d, const int8_t* const* llr, uint8_t* const
         if (ok || it >= max_iter)
             break;
         for (int f = 0; f < n; f++)
-            update(d, &l[f], it == 0);
+            update(d, &l[f], it == 0, NULL, NULL);
         it++;
     }
     for (int f = 0; f < n; f++) {
@@ -318,6 +331,34 @@ void orc_decode_frames(const orc_code* d, const int8_t* llr, uint8_t* out, int32
                                           max_iter, &it);
         iters[f] = it;
     }
+}
+
+/*
+ * This project's learned decoder at int8 (not in the reference): the same
+ * schedule with the node magnitude of learned_mag from row min(it, T - 1)
+ * of tab (8 words per row, one per degree class; cls[deg] is the class of a
+ * node of degree deg).  One frame, per-frame stopping; returns 1 if the
+ * syndrome passed.
+ */
+int orc_decode_frame_learned(const orc_code* d, const int8_t* llr, uint8_t* out, int max_iter, int* iters,
+                             const uint32_t* tab, int T, const int8_t* cls)
+{
+    lane l;
+    if (!lane_alloc(d, &l))
+        return -2;
+    lane_load(d, &l, llr);
+    int it = 0, ok;
+    for (;;) {
+        ok = !bad(d, l.data, l.pty);
+        if (ok || it >= max_iter)
+            break;
+        update(d, &l, it == 0, tab + 8 * (it < T ? it : T - 1), cls);
+        it++;
+    }
+    lane_store(d, &l, out);
+    lane_release(&l);
+    *iters = it;
+    return ok;
 }
 
 /*

@@ -1,0 +1,109 @@
+"""The learned min-sum decoder at int8 (drx_ldpc_set_learned,
+drx_ldpc_decode_learned_device) through the C ABI: with scale 1 and
+offset 1 it is the plain decoder bit for bit; with other tables it matches
+the CPU model of the learned rule bit for bit (bits, iterations, flags) on
+both kernels; the fallback hands exactly the failing frames to the plain
+decoder."""
+import numpy as np
+import pytest
+import torch
+
+import dvbrx_b200 as D
+import oracle
+from helpers import awgn_frames
+
+pytestmark = pytest.mark.gpu
+
+
+def classes(short, rate):
+    from dvbrx_b200 import learned as Lm
+
+    degs, cod = Lm.degree_classes(short, rate)
+    return len(degs), cod
+
+
+def random_tables(iters, nclass, seed):
+    rng = np.random.default_rng(seed)
+    scale = rng.uniform(0.55, 1.25, size=(iters, nclass)).astype(np.float32)
+    offset = rng.uniform(-0.75, 2.5, size=(iters, nclass)).astype(np.float32)
+    return scale, offset
+
+
+def variants(dec):
+    out = [D.VARIANT_FRAME]
+    if dec.set_variant(D.VARIANT_AUTO) == D.VARIANT_PAIR:
+        out.append(D.VARIANT_PAIR)
+    return out
+
+
+@pytest.mark.parametrize("short,rate,es", [(1, "1_2", 1.5), (0, "3_5", 2.6), (0, "9_10", 6.6), (1, "8_9", 6.2)])
+def test_unit_table_is_plain(short, rate, es):
+    dec = D.Ldpc(D.fec_lookup(short, rate), rate)
+    n = 40
+    llr = torch.from_numpy(awgn_frames(short, rate, n, es, seed=3)).cuda()
+    nclass, cod = classes(short, rate)
+    dec.set_learned(np.ones((30, nclass)), np.ones((30, nclass)), cod)
+    for v in variants(dec):
+        dec.set_variant(v)
+        want = dec.decode_device(llr, 30)
+        got = dec.decode_learned(llr, 30, 0)
+        torch.cuda.synchronize()
+        for w, g in zip(want, got[:3]):
+            assert torch.equal(w, g), (rate, v)
+        assert int(got[3].sum()) == 0
+
+
+@pytest.mark.parametrize("short,rate,es,iters", [(1, "1_2", 1.6, 8), (0, "3_5", 2.7, 6), (0, "2_3", 3.2, 7),
+                                                 (1, "8_9", 6.3, 9)])
+def test_random_tables_match_cpu_model(short, rate, es, iters):
+    dec = D.Ldpc(D.fec_lookup(short, rate), rate)
+    n = 24 if short else 8
+    llr_np = awgn_frames(short, rate, n, es, seed=11)
+    llr = torch.from_numpy(llr_np).cuda()
+    nclass, cod = classes(short, rate)
+    scale, offset = random_tables(iters, nclass, seed=iters)
+    dec.set_learned(scale, offset, cod)
+    want = oracle.OrcCode(short, rate).decode_frames_learned(llr_np, iters, scale, offset, cod)
+    for v in variants(dec):
+        dec.set_variant(v)
+        bits, it, ok, fb = dec.decode_learned(llr, iters, 0)
+        assert np.array_equal(bits.cpu().numpy(), want[0]), (rate, v)
+        assert np.array_equal(it.cpu().numpy(), want[1]), (rate, v)
+        assert np.array_equal(ok.cpu().numpy(), want[2]), (rate, v)
+
+
+@pytest.mark.parametrize("short,rate,es,iters,n", [(1, "1_2", 1.4, 8, 64), (0, "3_5", 2.6, 11, 32)])
+def test_fallback_redecodes_failing_frames(short, rate, es, iters, n):
+    dec = D.Ldpc(D.fec_lookup(short, rate), rate)
+    llr = torch.from_numpy(awgn_frames(short, rate, n, es, seed=5)).cuda()
+    nclass, cod = classes(short, rate)
+    dec.set_learned(np.full((iters, nclass), 0.875), np.full((iters, nclass), 0.25), cod)
+    for v in variants(dec):
+        dec.set_variant(v)
+        lb, li, lo, _ = dec.decode_learned(llr, iters, 0)
+        pb, pi, po = dec.decode_device(llr, 30)
+        bits, it, ok, fb = dec.decode_learned(llr, iters, 30)
+        torch.cuda.synchronize()
+        fail = lo == 0
+        assert 0 < int(fail.sum()) < n, "the case should mix converged and failing frames"
+        assert torch.equal(fb.bool(), fail)
+        keep = ~fail
+        assert torch.equal(bits[keep], lb[keep]) and torch.equal(it[keep], li[keep])
+        assert bool((ok[keep] == 1).all())
+        assert torch.equal(bits[fail], pb[fail]) and torch.equal(it[fail], pi[fail])
+        assert torch.equal(ok[fail], po[fail])
+
+
+def test_set_learned_errors():
+    dec = D.Ldpc(D.fec_lookup(1, "1_2"), "1_2")
+    llr = torch.zeros((2, dec.N), dtype=torch.int8, device="cuda")
+    with pytest.raises(RuntimeError):
+        dec.decode_learned(llr, 5)  # no table yet
+    with pytest.raises(RuntimeError):
+        dec.set_learned(np.ones((33, 1)), np.ones((33, 1)), np.zeros(33, np.int8))  # > 32 iterations
+    with pytest.raises(RuntimeError):
+        dec.set_learned(np.ones((4, 1)), np.ones((4, 1)), np.full(33, 1, np.int8))  # class out of range
+    dec.set_learned(np.ones((4, 1)), np.ones((4, 1)), np.zeros(33, np.int8))
+    dec.set_learned(None, None, None)
+    with pytest.raises(RuntimeError):
+        dec.decode_learned(llr, 5)

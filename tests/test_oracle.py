@@ -114,3 +114,26 @@ def test_demapper_matches_reference():
     lib.ref_demap_free(d)
     diff = np.abs(mine.astype(int) - theirs.astype(int))
     assert diff.max() <= 1 and (diff == 0).mean() > 0.99
+
+
+def test_learned_model_unit_table_is_plain():
+    """The CPU model of the learned int8 decoder with scale 1 and offset 1
+    in every class and iteration is the plain decoder, bit for bit."""
+    code = oracle.OrcCode(1, "1_2")
+    fr = oracle.datagen.make_frames(1, "1_2", 24, 1.4, seed=21, code=code)
+    cls = np.zeros(33, np.int8)
+    ones = np.ones((50, 1), np.float32)
+    want = code.decode_frames(fr["llr"], 50)
+    got = code.decode_frames_learned(fr["llr"], 50, ones[:32], ones[:32], cls)
+    for w, g in zip(want, got):
+        assert np.array_equal(w, g)
+
+
+def test_learned_words_rounding():
+    """Q8 words: round half to even, clamped scale and offset."""
+    w = oracle.learned_words([[1.0, 0.5 / 256, 300.0, -1.0]], [[1.0, -0.5, 200.0, -200.0]])
+    assert w.shape == (1, 8)
+    assert w[0, 0] == (256 | 256 << 16)
+    assert w[0, 1] & 0xFFFF == 0 and (w[0, 1] >> 16) == (0x10000 - 128)  # 0.5 -> 0 (half-even), -0.5 -> -128
+    assert w[0, 2] & 0xFFFF == 65535 and (w[0, 2] >> 16) == 32767
+    assert w[0, 3] & 0xFFFF == 0 and (w[0, 3] >> 16) == 0x8000

@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(kLT) k_learned_bwd(LearnedParams p)
         }
         load_params(p, t, sbeta, salpha);
         iteration_fwd(c, s, p, t, sbeta, salpha); /* saves X */
-        iteration_loss(c, s, p, f, p.loss_scale);
+        iteration_loss(c, s, p, f, p.loss_scale * (p.loss_w ? p.loss_w[t] : 1.0f));
         __syncthreads();
         float db[kLearnedMaxClass], da[kLearnedMaxClass];
         for (int k = 0; k < p.nclass; k++)

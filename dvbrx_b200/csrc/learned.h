@@ -39,6 +39,7 @@ struct LearnedParams {
     float* dbeta;        /* backward: iters x nclass */
     float* dalpha;
     float loss_scale;    /* backward: d loss / d (each per-iteration BCE sum) */
+    const float* loss_w; /* backward, optional: per-iteration weights of the BCE sums (device) */
     float* post;         /* forward, optional: nframes x kldpc final posteriors */
 };
 

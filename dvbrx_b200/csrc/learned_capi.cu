@@ -140,8 +140,9 @@ int drx_learned_forward(drx_ldpc* d, int nframes, const void* llr_f16, size_t ll
 
 int drx_learned_backward(drx_ldpc* d, int nframes, const void* llr_f16, size_t llr_stride, const uint8_t* bits,
                          size_t bits_stride, int iters, const void* beta_f16, const void* alpha_f16, int nclass,
-                         const int8_t* class_of_degree, float loss_scale, float* dbeta, float* dalpha,
-                         float* loss_scratch, void* workspace, size_t workspace_bytes, void* stream)
+                         const int8_t* class_of_degree, float loss_scale, const float* iter_weights,
+                         float* dbeta, float* dalpha, float* loss_scratch, void* workspace,
+                         size_t workspace_bytes, void* stream)
 {
     cudaStream_t s = stream ? (cudaStream_t)stream : (d ? d->stream : nullptr);
     LearnedParams p;
@@ -154,6 +155,7 @@ int drx_learned_backward(drx_ldpc* d, int nframes, const void* llr_f16, size_t l
     }
     p.loss = loss_scratch;
     p.loss_scale = loss_scale;
+    p.loss_w = iter_weights;
     p.dbeta = dbeta;
     p.dalpha = dalpha;
     return cuda_check(launch_learned(p, true, s), "learned backward") ? 0 : -1;

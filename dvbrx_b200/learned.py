@@ -37,7 +37,7 @@ def _bind():
     L.drx_learned_workspace_bytes.restype = sz
     L.drx_learned_forward.argtypes = [vp, ip, vp, sz, vp, sz, ip, vp, vp, ip, vp, vp, vp, vp, sz, ip, vp]
     L.drx_learned_forward.restype = ip
-    L.drx_learned_backward.argtypes = [vp, ip, vp, sz, vp, sz, ip, vp, vp, ip, vp, fp, vp, vp, vp, vp, sz, vp]
+    L.drx_learned_backward.argtypes = [vp, ip, vp, sz, vp, sz, ip, vp, vp, ip, vp, fp, vp, vp, vp, vp, vp, sz, vp]
     L.drx_learned_backward.restype = ip
     L.drx_ldpc_schedule.argtypes = [ip, ctypes.c_char_p, ctypes.POINTER(ip), ctypes.POINTER(ip), vp, vp]
     L.drx_ldpc_schedule.restype = ip
@@ -73,18 +73,24 @@ def degree_classes(short_frame, rate):
 
 
 class _Work:
-    """Workspace and class table of one (decoder, batch size, iterations)."""
+    """Workspace, class table and per-iteration loss weights of one
+    (decoder, batch size, iterations); weights None: all ones."""
 
-    def __init__(self, dec, nframes, iters, cod):
+    def __init__(self, dec, nframes, iters, cod, weights=None):
         L = _bind()
         self.bytes = L.drx_learned_workspace_bytes(dec.h, nframes, iters, 1)
         self.ws = torch.empty(self.bytes, dtype=torch.uint8, device="cuda")
         self.cod = np.ascontiguousarray(cod, dtype=np.int8)
+        w = np.ones(iters, np.float32) if weights is None else np.asarray(weights, np.float32)
+        assert w.shape == (iters,)
+        self.w = torch.from_numpy(w).cuda()
+        self.wsum = float(w.sum())
 
 
 class LearnedMinSum(torch.autograd.Function):
-    """Mean per-iteration BCE of the learned decoder over a batch; gradients
-    for the scale and offset tables through the hand-written backward."""
+    """Weighted mean of the per-iteration BCE of the learned decoder over a
+    batch (weights from the workspace, all ones by default); gradients for
+    the scale and offset tables through the hand-written backward."""
 
     @staticmethod
     def forward(ctx, beta, alpha, dec, llr16, bits, iters, cod, work):
@@ -101,9 +107,9 @@ class LearnedMinSum(torch.autograd.Function):
         if r:
             raise RuntimeError("drx_learned_forward: " + last_error())
         ctx.args = (dec, llr16, bits, iters, work, b16, a16, nclass, n)
-        denom = float(iters * n * dec.kldpc)
+        denom = work.wsum * n * dec.kldpc
         ctx.denom = denom
-        return loss.sum() / denom
+        return (loss * work.w).sum() / denom
 
     @staticmethod
     def backward(ctx, g):
@@ -116,7 +122,8 @@ class LearnedMinSum(torch.autograd.Function):
         s = torch.cuda.current_stream()
         r = L.drx_learned_backward(dec.h, n, llr16.data_ptr(), llr16.stride(0), bits.data_ptr(), bits.stride(0),
                                    iters, b16.data_ptr(), a16.data_ptr(), nclass, work.cod.ctypes.data,
-                                   ctypes.c_float(scale), dbeta.data_ptr(), dalpha.data_ptr(), scratch.data_ptr(),
+                                   ctypes.c_float(scale), work.w.data_ptr(), dbeta.data_ptr(), dalpha.data_ptr(),
+                                   scratch.data_ptr(),
                                    work.ws.data_ptr(), work.bytes, stream_handle(s))
         if r:
             raise RuntimeError("drx_learned_backward: " + last_error())
@@ -148,7 +155,7 @@ class LearnedDecoder(torch.nn.Module):
     fp32 masters of the FP16 values the decoder uses; initialised to the
     plain decoder (scale 1, offset 1)."""
 
-    def __init__(self, short_frame, rate, iters=20, params=None):
+    def __init__(self, short_frame, rate, iters=20, params=None, weights=None):
         super().__init__()
         from . import FecParams, code_info, fec_lookup
         try:
@@ -163,12 +170,13 @@ class LearnedDecoder(torch.nn.Module):
         self.beta = torch.nn.Parameter(torch.ones(iters, nclass, device="cuda"))
         self.alpha = torch.nn.Parameter(torch.ones(iters, nclass, device="cuda"))
         self._work = {}
+        self.weights = weights
 
     def forward(self, llr16, bits):
         n = llr16.shape[0]
         key = n
         if key not in self._work:
-            self._work[key] = _Work(self.dec, n, self.iters, self.cod)
+            self._work[key] = _Work(self.dec, n, self.iters, self.cod, self.weights)
         return LearnedMinSum.apply(self.beta, self.alpha, self.dec, llr16, bits, self.iters, self.cod,
                                    self._work[key])
 

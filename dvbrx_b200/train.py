@@ -1,0 +1,257 @@
+"""Train the learned (neural offset / scaled) min-sum decoder on the GPU and
+evaluate it against the plain decoder.
+
+    python -m dvbrx_b200.train --rate 2_3 --iters 20 --batch 512 --es 6.0 7.5 --steps 300 \\
+        --out table.json
+    python -m dvbrx_b200.train --eval table.json --es-list 6.0 6.25 6.5 --frames 4096
+
+Training data: the library's own frame generator (random information bits,
+the DVB-S2 encoder, the MODCOD's constellation and interleaver, AWGN, the
+max-log demapper) with FP16 LLRs on the int8 decoder's scale (2 x LLR,
+unquantised); every minibatch is drawn in chunks, each at its own Es/N0
+uniform in the given range.  Loss: mean binary cross-entropy of the
+information-bit posteriors after every unrolled iteration, through the
+hand-written forward and backward kernels (learned.LearnedMinSum).
+
+The exported table (JSON: scale and offset [iters][classes], the class of
+every check degree) is what Ldpc.set_learned / drx_ldpc_set_learned load;
+the int8 decoders round it to Q8.
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+import torch
+
+from . import FecParams, Ldpc, code_info, fec_lookup
+from .learned import LearnedDecoder, degree_classes, learned_posteriors
+
+TABLES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "learned_tables")
+
+
+def table_path(short_frame, rate, constellation, iters):
+    return os.path.join(TABLES, "%s_%s_%s_%dit.json" % ("short" if short_frame else "normal", rate,
+                                                        constellation.lower(), iters))
+
+
+def load_table(short_frame, rate, constellation, iters):
+    """A committed learned table, or None."""
+    path = table_path(short_frame, rate, constellation, iters)
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+def apply_table(dec, table):
+    """Load a table (dict as exported) into a decoder handle."""
+    dec.set_learned(np.asarray(table["scale"], np.float32), np.asarray(table["offset"], np.float32),
+                    np.asarray(table["class_of_degree"], np.int8))
+
+
+def _params(short_frame, rate):
+    try:
+        return fec_lookup(short_frame, rate)
+    except KeyError:
+        info = code_info(short_frame, rate)
+        return FecParams(int(bool(short_frame)), info.nldpc, info.K, info.K, 0)
+
+
+def minibatch(dec, n, es_lo, es_hi, constellation, rng, chunks=8):
+    """n frames in `chunks` groups, each at an Es/N0 drawn uniformly in
+    [es_lo, es_hi]: (FP16 LLRs [n, N], packed information bits [n, nbytes])."""
+    sizes = [n // chunks + (1 if k < n % chunks else 0) for k in range(chunks)]
+    llrs, infos = [], []
+    for s in sizes:
+        if s == 0:
+            continue
+        es = float(rng.uniform(es_lo, es_hi))
+        _, info, h = dec.generate(s, es, seed=int(rng.integers(1, 2**62)), constellation=constellation, llr=False,
+                                  info=True, llr_f16=True)
+        llrs.append(h)
+        infos.append(info)
+    return torch.cat(llrs), torch.cat(infos)
+
+
+def loss_weights(kind, iters):
+    """Per-iteration weights of the BCE sums: "uniform", "ramp" ((t + 1) / T)
+    or "last" (the final iteration only)."""
+    if kind == "uniform":
+        return np.ones(iters, np.float32)
+    if kind == "ramp":
+        return (np.arange(iters, dtype=np.float32) + 1) / iters
+    if kind == "last":
+        w = np.zeros(iters, np.float32)
+        w[-1] = 1.0
+        return w
+    raise ValueError(kind)
+
+
+def validation_set(dec, es_points, n, constellation, seed=99):
+    """Fixed frames: one (FP16 LLRs, info bits) pair per Es/N0 point."""
+    out = []
+    for k, es in enumerate(es_points):
+        _, info, h = dec.generate(n, float(es), seed=seed + k, constellation=constellation, llr=False, info=True,
+                                  llr_f16=True)
+        out.append((float(es), h, info))
+    return out
+
+
+def validate(model, vset):
+    """Per Es/N0 point: mean BCE of the last iteration and the FER of the
+    float model's final hard decisions."""
+    b, a = model.fp16_tables()
+    res = []
+    for es, h, info in vset:
+        loss, post = learned_posteriors(model.dec, b, a, model.cod, h, info, model.iters)
+        bits = torch.from_numpy(np.unpackbits(info.cpu().numpy(), axis=1)[:, : model.dec.kldpc]).cuda()
+        err = ((post < 0).to(torch.uint8) != bits).any(dim=1).float().mean()
+        res.append({"esn0_db": es, "bce_last": float(loss[-1]) / (h.shape[0] * model.dec.kldpc),
+                    "float_fer": float(err)})
+    return res
+
+
+def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, lr, seed, log=None,
+          weights="uniform", val_points=None):
+    """Adam on the fp32 masters of the FP16 tables, initialised to the
+    plain decoder (scale 1, offset 1).  Returns (model, history)."""
+    torch.manual_seed(seed)
+    rng = np.random.default_rng(seed)
+    model = LearnedDecoder(short_frame, rate, iters=iters, params=_params(short_frame, rate),
+                           weights=loss_weights(weights, iters))
+    vset = validation_set(model.dec, val_points or [es_lo, (es_lo + es_hi) / 2, es_hi], 256, constellation)
+    if log:
+        log(json.dumps({"validation_init": validate(model, vset)}))
+    opt = torch.optim.Adam(model.parameters(), lr=lr)
+    hist = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in range(steps):
+        llr16, info = minibatch(model.dec, batch, es_lo, es_hi, constellation, rng)
+        torch.cuda.synchronize()
+        ev0.record()
+        loss = model(llr16, info)
+        opt.zero_grad()
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            model.beta.clamp_(0.0, 4.0)
+        ev1.record()
+        torch.cuda.synchronize()
+        rec = {"step": k, "loss": float(loss.detach()), "ms": ev0.elapsed_time(ev1)}
+        hist.append(rec)
+        if log and (k % 10 == 0 or k == steps - 1):
+            log(json.dumps(rec))
+    model.validation = validate(model, vset)
+    if log:
+        log(json.dumps({"validation_final": model.validation}))
+    return model, hist
+
+
+def export(model, meta):
+    b, a = model.fp16_tables()
+    t = dict(meta)
+    t.update({"iters": model.iters, "degrees": model.degrees, "class_of_degree": [int(v) for v in model.cod],
+              "scale": b.float().cpu().numpy().tolist(), "offset": a.float().cpu().numpy().tolist()})
+    return t
+
+
+def evaluate(short_frame, rate, constellation, table, es_list, nframes, learned_iters, plain_iters, seed=7):
+    """FER of plain@plain_iters, plain@learned_iters, learned@learned_iters
+    and learned + plain fallback on the same frames, with device-timed
+    Gbit/s of the plain and the learned + fallback decodes."""
+    p = _params(short_frame, rate)
+    dec = Ldpc(p, rate)
+    apply_table(dec, table)
+    rows = []
+    for k, es in enumerate(es_list):
+        llr, info, _ = dec.generate(nframes, float(es), seed=seed + 1000 * k, constellation=constellation, info=True)
+        res = {"esn0_db": float(es)}
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        dec.decode_device(llr, plain_iters)  # warm-up
+        dec.decode_learned(llr, learned_iters, plain_iters)
+        torch.cuda.synchronize()
+        ev[0].record()
+        pb, pi, po = dec.decode_device(llr, plain_iters)
+        ev[1].record()
+        lb, li, lo, fb = dec.decode_learned(llr, learned_iters, plain_iters)
+        ev[2].record()
+        torch.cuda.synchronize()
+        sb, si, so = dec.decode_device(llr, learned_iters)
+        ob, oi, oo, _ = dec.decode_learned(llr, learned_iters, 0)
+        torch.cuda.synchronize()
+
+        def fer(bits):
+            return float((bits != info).any(dim=1).float().mean())
+
+        def ber(bits):
+            x = torch.bitwise_xor(bits, info)
+            ones = sum(int(((x >> b) & 1).sum()) for b in range(8))
+            return ones / float(nframes * p.kldpc)
+
+        t_plain = ev[0].elapsed_time(ev[1]) * 1e-3
+        t_learn = ev[1].elapsed_time(ev[2]) * 1e-3
+        res.update({
+            "plain_fer": fer(pb), "plain_ber": ber(pb), "plain_avg_iters": float(pi.float().mean()),
+            "plain_short_fer": fer(sb),
+            "learned_only_fer": fer(ob), "learned_only_avg_iters": float(oi.float().mean()),
+            "learned_fer": fer(lb), "learned_ber": ber(lb), "fallback_frac": float(fb.float().mean()),
+            "plain_gbps": nframes * p.kldpc / t_plain / 1e9, "learned_gbps": nframes * p.kldpc / t_learn / 1e9,
+        })
+        rows.append(res)
+    return rows
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--short", type=int, default=0)
+    ap.add_argument("--rate", default="2_3")
+    ap.add_argument("--const", default="8PSK")
+    ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=512)
+    ap.add_argument("--es", type=float, nargs=2, default=[6.0, 7.5])
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--lr", type=float, default=0.02)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", default=None, help="table JSON (default: the package's table path)")
+    ap.add_argument("--eval", default=None, help="evaluate this table JSON instead of training")
+    ap.add_argument("--es-list", type=float, nargs="*", default=None)
+    ap.add_argument("--frames", type=int, default=2048)
+    ap.add_argument("--plain-iters", type=int, default=30)
+    ap.add_argument("--weights", default="uniform", choices=["uniform", "ramp", "last"])
+    ap.add_argument("--val", type=float, nargs="*", default=None, help="validation Es/N0 points")
+    a = ap.parse_args(argv)
+    log = lambda s: print(s, flush=True)
+    if a.eval:
+        with open(a.eval) as f:
+            table = json.load(f)
+        es_list = a.es_list or list(np.arange(table["es"][0], table["es"][1] + 1e-6, 0.25))
+        rows = evaluate(table["short"], table["rate"], table["constellation"], table, es_list, a.frames,
+                        table["iters"], a.plain_iters)
+        for r in rows:
+            log(json.dumps(r))
+        return 0
+    t0 = time.time()
+    model, hist = train(a.short, a.rate, a.const, a.iters, a.batch, a.es[0], a.es[1], a.steps, a.lr, a.seed, log,
+                        a.weights, a.val)
+    wall = time.time() - t0
+    ms = [h["ms"] for h in hist[1:]] or [hist[0]["ms"]]
+    meta = {"short": a.short, "rate": a.rate, "constellation": a.const, "es": a.es, "batch": a.batch,
+            "steps": a.steps, "lr": a.lr, "seed": a.seed, "weights": a.weights,
+            "validation": model.validation,
+            "loss_first": hist[0]["loss"], "loss_last": float(np.mean([h["loss"] for h in hist[-10:]])),
+            "train_ms_per_step": float(np.median(ms)), "train_frames_per_s": a.batch / (float(np.median(ms)) * 1e-3),
+            "train_wall_s": wall}
+    table = export(model, meta)
+    out = a.out or table_path(a.short, a.rate, a.const, a.iters)
+    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+    with open(out, "w") as f:
+        json.dump(table, f, indent=1)
+    log(json.dumps({k: v for k, v in meta.items()}))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -205,12 +205,14 @@ int drx_learned_forward(drx_ldpc* d, int nframes, const void* llr_f16, size_t ll
 
 /* Backward of a training forward with the same arguments and workspace:
  * adds to dbeta and dalpha (device fp32, iters x nclass) the gradient of
- * loss_scale x (sum of the per-iteration BCE sums).  loss_scratch: device
- * float[iters] the re-run forward writes into. */
+ * loss_scale x (sum over t of w[t] x the BCE sum of iteration t), with
+ * w = iter_weights (device float[iters]) or all ones if NULL.
+ * loss_scratch: device float[iters] the re-run forward writes into. */
 int drx_learned_backward(drx_ldpc* d, int nframes, const void* llr_f16, size_t llr_stride, const uint8_t* bits,
                          size_t bits_stride, int iters, const void* beta_f16, const void* alpha_f16, int nclass,
-                         const int8_t* class_of_degree, float loss_scale, float* dbeta, float* dalpha,
-                         float* loss_scratch, void* workspace, size_t workspace_bytes, void* stream);
+                         const int8_t* class_of_degree, float loss_scale, const float* iter_weights,
+                         float* dbeta, float* dalpha, float* loss_scratch, void* workspace,
+                         size_t workspace_bytes, void* stream);
 
 /* ---- learned min-sum: int8 inference --------------------------------------
  *

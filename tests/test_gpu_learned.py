@@ -12,7 +12,7 @@ from dvbrx_b200 import learned as Lm
 pytestmark = pytest.mark.gpu
 
 
-def reference_loss(short, rate, llr, bits, beta, alpha, iters, cod):
+def reference_loss(short, rate, llr, bits, beta, alpha, iters, cod, weights=None):
     """The learned decoder in torch (float64): same schedule (steps of the
     library's wavefront levels), same saturations, autograd gradients."""
     step, links = Lm.schedule(short, rate)
@@ -26,6 +26,7 @@ def reference_loss(short, rate, llr, bits, beta, alpha, iters, cod):
     b = torch.from_numpy(bits).to(llr.device)
     sgnb = 1.0 - 2.0 * b.double()
     total = 0.0
+    w = np.ones(iters) if weights is None else np.asarray(weights, np.float64)
     for t in range(iters):
         Mn = M.clone()
         for chk in groups:
@@ -53,9 +54,9 @@ def reference_loss(short, rate, llr, bits, beta, alpha, iters, cod):
             Mn[:, ck, :] = torch.where(valid, m.clamp(-32, 31), torch.zeros_like(m))
             del deg
         M = Mn
-        total = total + torch.nn.functional.softplus(-sgnb * P[:, :kl] / 2).sum()
+        total = total + float(w[t]) * torch.nn.functional.softplus(-sgnb * P[:, :kl] / 2).sum()
     del K
-    return total / (iters * n * kl)
+    return total / (float(w.sum()) * n * kl)
 
 
 def small_case(short, rate, n, es, iters, seed):
@@ -66,7 +67,8 @@ def small_case(short, rate, n, es, iters, seed):
     return dec, llr16, info, bits
 
 
-def test_backward_matches_float_reference():
+@pytest.mark.parametrize("weights", [None, [0.0, 0.5, 2.0]])
+def test_backward_matches_float_reference(weights):
     short, rate, iters = 1, "1_2", 3
     dec, llr16, info, bits = small_case(short, rate, 3, 1.2, iters, 5)
     degs, cod = Lm.degree_classes(short, rate)
@@ -77,15 +79,15 @@ def test_backward_matches_float_reference():
 
     beta = beta0.clone().requires_grad_(True)
     alpha = alpha0.clone().requires_grad_(True)
-    work = Lm._Work(dec, llr16.shape[0], iters, cod)
+    work = Lm._Work(dec, llr16.shape[0], iters, cod, weights)
     loss = Lm.LearnedMinSum.apply(beta, alpha, dec, llr16, info, iters, cod, work)
     loss.backward()
 
     rb = beta0.double().clone().requires_grad_(True)
     ra = alpha0.double().clone().requires_grad_(True)
-    rl = reference_loss(short, rate, llr16.double(), bits, rb, ra, iters, cod)
+    rl = reference_loss(short, rate, llr16.double(), bits, rb, ra, iters, cod, weights)
     rl.backward()
-    assert abs(float(loss) - float(rl)) <= 1e-4 * abs(float(rl)) + 1e-6
+    assert abs(float(loss.detach()) - float(rl.detach())) <= 1e-4 * abs(float(rl.detach())) + 1e-6
     for got, want in ((beta.grad, rb.grad), (alpha.grad, ra.grad)):
         want = want.float()
         err = (got - want).norm() / want.norm()

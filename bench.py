@@ -36,6 +36,7 @@ sys.path.insert(0, ROOT)
 METRIC = "LDPC info Gbit/s at matched FER: learned vs plain min-sum, 1xB200 vs host CPU"
 UNIT = "Gbit/s"
 RATE, SHORT, CONST = "3_5", 0, "8PSK"
+LEARNED_ITERS = 12
 ESN0 = [5.0, 5.25, 5.5, 5.75, 6.0, 6.25, 6.5]
 MAX_ITER = 30
 SMEM_BYTES_PER_CLK = 128  # per SM
@@ -51,6 +52,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--e2e-steps", type=int, default=7)
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned decoder's line items")
     ap.add_argument("--variant", default="auto", choices=["auto", "frame"],
                     help="decoder kernel: automatic choice, or the one-frame kernel")
     ap.add_argument("--batches", type=int, default=len(ESN0),
@@ -122,6 +124,12 @@ class ClockSampler:
                 "sm_max_mhz": max(smax) if smax else None,
                 "samples": len(sm),
                 "reasons": sorted(reasons)}
+
+
+def load_learned_table():
+    """The committed learned table of the workload's code, or None."""
+    from dvbrx_b200 import train as T
+    return T.load_table(SHORT, RATE, CONST, LEARNED_ITERS)
 
 
 def profiled_figures():
@@ -366,6 +374,50 @@ def run_b200(args):
         "sm_mhz_median": sm_mhz,
     }
 
+    # the learned decoder (committed 12-iteration table, int8) with the plain
+    # decoder as fallback, on the same batches and steps
+    learned = None
+    table = None if args.no_learned else load_learned_table()
+    if table is not None:
+        from dvbrx_b200 import train as T
+        T.apply_table(dec, table)
+        L = int(table["iters"])
+        l_it = [torch.empty(F, dtype=torch.int32, device="cuda") for _ in range(args.steps)]
+        l_ok = [torch.empty(F, dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
+        l_fb = [torch.empty(F, dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
+        for k in range(args.warmup):
+            dec.decode_learned(llr[k % len(llr)], L, MAX_ITER, out=outs[0], iters=l_it[0], ok=l_ok[0],
+                               fallback=l_fb[0])
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        lev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            lev[k][0].record(stream)
+            dec.decode_learned(llr[(args.warmup + k) % len(llr)], L, MAX_ITER, out=outs[k], iters=l_it[k],
+                               ok=l_ok[k], fallback=l_fb[k])
+            lev[k][1].record(stream)
+        torch.cuda.synchronize()
+        l_ms = lev[0][0].elapsed_time(lev[-1][1])
+        t = torch.tensor([l_ms], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        l_ms = float(t.item())
+        l_err = sum(int((outs[k] != info[(args.warmup + k) % len(info)]).any(dim=1).sum()) for k in range(args.steps))
+        fb_all = torch.stack(l_fb).float()
+        lval = world * frames_rank * kldpc / (l_ms * 1e-3) / 1e9
+        learned = {
+            "value": lval, "unit": UNIT, "vs_plain": lval / value, "fer": l_err / frames_rank, "plain_fer": fer,
+            "fallback_frac": float(fb_all.mean()),
+            "avg_iterations_learned_pass": float(torch.stack(l_it).float()[fb_all == 0].mean()) if bool((fb_all == 0).any()) else None,
+            "learned_iters": L, "plain_fallback_max_iter": MAX_ITER, "ms_per_step": l_ms / args.steps,
+            "table": "dvbrx_b200/learned_tables/" + os.path.basename(T.table_path(SHORT, RATE, CONST, L)),
+            "launches_per_step": 3,
+            "decoder": "learned scaled/offset min-sum at int8 (Q8 table per iteration and degree class), "
+                       "frames failing the syndrome re-decoded by the plain decoder on the device",
+        }
+        dec.set_learned(None, None, None)
+
     # end to end through the C ABI with host buffers (synchronous call)
     e2e = None
     if args.e2e_steps > 0:
@@ -410,7 +462,7 @@ def run_b200(args):
             "config": workload_config(F, world),
             "decoder": "plain layered offset min-sum (bit-exact to the reference)",
             "quality": {"fer": fer, "avg_iterations": iters_sum / frames_rank},
-            "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+            "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "learned": learned,
             "gpu_launches": args.steps,
         }
         print(json.dumps(line))

@@ -101,6 +101,10 @@ def lib():
         L.drx_ldpc_set_variant.restype = ip
         L.drx_ldpc_device_error.argtypes = [vp]
         L.drx_ldpc_device_error.restype = ip
+        L.drx_ldpc_mix_set_learned.argtypes = [vp, ip, ip, ip, vp, vp, vp]
+        L.drx_ldpc_mix_set_learned.restype = ip
+        L.drx_ldpc_mix_plan_learned.argtypes = [vp, ip, vp, vp, sz, vp, sz, vp, vp, vp, ip, ip]
+        L.drx_ldpc_mix_plan_learned.restype = ip
         L.drx_ldpc_set_learned.argtypes = [vp, ip, ip, vp, vp, vp]
         L.drx_ldpc_set_learned.restype = ip
         L.drx_ldpc_decode_learned_device.argtypes = [vp, vp, sz, vp, sz, vp, vp, vp, ip, ip, ip, vp]
@@ -354,6 +358,29 @@ class LdpcMix:
         if r != 0:
             raise RuntimeError("drx_ldpc_mix_plan: " + last_error())
         self._keep = (llr, out, iters, ok)
+
+    def set_learned(self, code_index, scale, offset, class_of_degree):
+        """``drx_ldpc_mix_set_learned``: learned tables of one code of the set."""
+        b = np.ascontiguousarray(np.asarray(scale, dtype=np.float32))
+        a = np.ascontiguousarray(np.asarray(offset, dtype=np.float32))
+        cod = np.ascontiguousarray(np.asarray(class_of_degree, dtype=np.int8))
+        r = self._lib.drx_ldpc_mix_set_learned(self.h, int(code_index), b.shape[0], b.shape[1], cod.ctypes.data,
+                                              b.ctypes.data, a.ctypes.data)
+        if r != 0:
+            raise RuntimeError("drx_ldpc_mix_set_learned: " + last_error())
+
+    def plan_learned(self, code, llr, out, iters, ok, fallback, learned_iters, plain_max_iter):
+        """``drx_ldpc_mix_plan_learned``: as plan, learned decode with the
+        plain decoder as fallback; fallback: torch CUDA uint8 [n] or None."""
+        code = np.ascontiguousarray(code, dtype=np.int32)
+        n = code.shape[0]
+        r = self._lib.drx_ldpc_mix_plan_learned(
+            self.h, n, code.ctypes.data, llr.data_ptr(), llr.stride(0), out.data_ptr(), out.stride(0),
+            iters.data_ptr(), ok.data_ptr(), fallback.data_ptr() if fallback is not None else None,
+            int(learned_iters), int(plain_max_iter))
+        if r != 0:
+            raise RuntimeError("drx_ldpc_mix_plan_learned: " + last_error())
+        self._keep = (llr, out, iters, ok, fallback)
 
     def set_tiling(self, tiling):
         if self._lib.drx_ldpc_mix_set_tiling(self.h, int(tiling)) < 0:

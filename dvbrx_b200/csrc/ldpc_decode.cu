@@ -465,13 +465,14 @@ __global__ void __launch_bounds__(kThreads, MINB) k_decode_mix(MixParams mp)
     DevCode c{};
     Frame fr{};
     int lT = 0;
+    const int nframes = mp.nframes_dev ? *mp.nframes_dev : mp.nframes;
     for (;;) {
         if (threadIdx.x == 0)
             s_k = (int)atomicAdd(mp.work, 1u);
         __syncthreads();
         const int k = s_k;
         __syncthreads();
-        if (k >= mp.nframes)
+        if (k >= nframes)
             break;
         const int ci = mp.frame_code[mp.order[k]];
         if (ci != staged) {
@@ -481,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_decode_mix(MixParams mp)
             staged = ci;
             __syncthreads();
         }
-        decode_frame<DMAX>(c, fr, p, mp.nframes, k, msg, &s_flag, nullptr, lT);
+        decode_frame<DMAX>(c, fr, p, nframes, k, msg, &s_flag, nullptr, lT);
     }
 }
 

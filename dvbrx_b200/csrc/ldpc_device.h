@@ -113,6 +113,7 @@ struct MixParams {
     const uint32_t* const* learn;
     const int8_t* const* learn_class;
     const int* learn_iters;
+    const int* nframes_dev; /* optional: the number of rows of `order`, read on the device */
 };
 
 /* One persistent launch over a mixed batch: one frame per CTA, the CTA

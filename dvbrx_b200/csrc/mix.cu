@@ -54,6 +54,13 @@ struct drx_ldpc_mix {
     int32_t* d_order = nullptr;
     unsigned* d_work = nullptr; /* one counter per code, then one for the one-launch kernel */
     void* d_msg = nullptr;
+    /* learned plans: per-code learned tables (device pointer arrays), the
+     * failing rows of the learned pass (nframes + a count) and flags */
+    const uint32_t** d_learn = nullptr;
+    const int8_t** d_learn_cls = nullptr;
+    int* d_learn_iters = nullptr;
+    int32_t* d_fb_rows = nullptr;
+    uint8_t* d_fb_ok = nullptr;
     cudaGraphExec_t exec[3] = {};
     int tiling = DRX_TILING_ONE_LAUNCH;
     float tuned_ms[3] = {};
@@ -72,6 +79,16 @@ void release_plan(drx_ldpc_mix* m)
     cudaFree(m->d_order);
     cudaFree(m->d_work);
     cudaFree(m->d_msg);
+    cudaFree(m->d_learn);
+    cudaFree(m->d_learn_cls);
+    cudaFree(m->d_learn_iters);
+    cudaFree(m->d_fb_rows);
+    cudaFree(m->d_fb_ok);
+    m->d_learn = nullptr;
+    m->d_learn_cls = nullptr;
+    m->d_learn_iters = nullptr;
+    m->d_fb_rows = nullptr;
+    m->d_fb_ok = nullptr;
     m->d_frame_code = m->d_order = nullptr;
     m->d_work = nullptr;
     m->d_msg = nullptr;
@@ -79,6 +96,59 @@ void release_plan(drx_ldpc_mix* m)
 }
 
 bool pair_runs(const drx_ldpc* h) { return h->variant != DRX_VARIANT_FRAME && h->pair_ctas_per_sm > 0; }
+
+constexpr int kCompactThreads = 1024;
+
+/* The rows of `order` whose flag in ok is 0, in `order`'s sequence (so a
+ * code's frames stay together), into rows; their number into *count and a
+ * flag per row into fallback (may be null).  One block: each thread scans a
+ * contiguous chunk, a block-wide exclusive scan places the chunks. */
+__global__ void __launch_bounds__(kCompactThreads) k_compact_failing(const int32_t* __restrict__ order,
+                                                                     const uint8_t* __restrict__ ok, int n,
+                                                                     int32_t* __restrict__ rows, int* count,
+                                                                     uint8_t* __restrict__ fallback)
+{
+    __shared__ int warp_sum[kCompactThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int chunk = (n + kCompactThreads - 1) / kCompactThreads;
+    const int b = min(n, t * chunk), e = min(n, b + chunk);
+    int mine = 0;
+    for (int k = b; k < e; k++) {
+        const int r = order[k];
+        const bool fail = ok[r] == 0;
+        if (fallback)
+            fallback[r] = fail ? 1 : 0;
+        mine += fail;
+    }
+    int x = mine; /* inclusive scan in the warp */
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        warp_sum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < kCompactThreads / 32 ? warp_sum[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o)
+                s += y;
+        }
+        if (lane < kCompactThreads / 32)
+            warp_sum[lane] = s; /* inclusive over warps */
+    }
+    __syncthreads();
+    int pos = x - mine + (w > 0 ? warp_sum[w - 1] : 0);
+    for (int k = b; k < e; k++) {
+        const int r = order[k];
+        if (ok[r] == 0)
+            rows[pos++] = r;
+    }
+    if (t == kCompactThreads - 1)
+        *count = pos;
+}
 
 }  // namespace
 
@@ -152,8 +222,17 @@ void drx_ldpc_mix_free(drx_ldpc_mix* m)
     delete m;
 }
 
-int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* llr, size_t llr_stride,
-                      uint8_t* out, size_t out_stride, int32_t* iters, uint8_t* ok, int max_iter)
+}  // extern "C"
+
+namespace {
+
+/* Plan (capture) both tilings of a mixed batch.  learned: the first pass
+ * runs every code's learned table for at most max_iter iterations, then the
+ * failing rows are gathered on the device and decoded again by the plain
+ * decoder (one launch, at most plain_max_iter iterations; none if <= 0). */
+int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* llr, size_t llr_stride,
+             uint8_t* out, size_t out_stride, int32_t* iters, uint8_t* ok, int max_iter, bool learned,
+             int plain_max_iter, uint8_t* fallback)
 {
     if (!m || nframes <= 0 || !code || !llr || !out) {
         set_error("drx_ldpc_mix_plan: bad arguments");
@@ -179,6 +258,12 @@ int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const i
     }
     if (max_iter < 0)
         max_iter = 0;
+    if (learned)
+        for (int c = 0; c < ncodes; c++)
+            if (count[c] && m->codes[c]->learn_iters <= 0) {
+                set_error("drx_ldpc_mix_plan_learned: a code of the batch has no learned table");
+                return -1;
+            }
     release_plan(m);
     /* longest work first: normal frames, then by edges; a code's frames together */
     std::vector<int> corder(ncodes);
@@ -239,6 +324,32 @@ int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const i
         release_plan(m);
         return -1;
     }
+    if (learned) {
+        std::vector<const uint32_t*> lt(ncodes, nullptr);
+        std::vector<const int8_t*> lc(ncodes, nullptr);
+        std::vector<int> li(ncodes, 0);
+        for (int c = 0; c < ncodes; c++) {
+            drx_ldpc* h = m->codes[c];
+            if (h->learn_iters > 0) {
+                lt[c] = h->learn;
+                lc[c] = (const int8_t*)((const char*)h->learn + sizeof(uint32_t) * kLearnMaxIters * kLearnClasses);
+                li[c] = h->learn_iters;
+            }
+        }
+        if (!cuda_check(cudaMalloc(&m->d_learn, sizeof(void*) * ncodes), "cudaMalloc") ||
+            !cuda_check(cudaMalloc(&m->d_learn_cls, sizeof(void*) * ncodes), "cudaMalloc") ||
+            !cuda_check(cudaMalloc(&m->d_learn_iters, sizeof(int) * ncodes), "cudaMalloc") ||
+            !cuda_check(cudaMalloc(&m->d_fb_rows, sizeof(int32_t) * (nframes + 4)), "cudaMalloc") ||
+            !cuda_check(cudaMalloc(&m->d_fb_ok, nframes), "cudaMalloc") ||
+            !cuda_check(cudaMemcpy(m->d_learn, lt.data(), sizeof(void*) * ncodes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
+            !cuda_check(cudaMemcpy(m->d_learn_cls, lc.data(), sizeof(void*) * ncodes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
+            !cuda_check(cudaMemcpy(m->d_learn_iters, li.data(), sizeof(int) * ncodes, cudaMemcpyHostToDevice), "cudaMemcpy")) {
+            release_plan(m);
+            return -1;
+        }
+        if (!ok)
+            ok = m->d_fb_ok;
+    }
     m->nframes = nframes;
     /* kernel attributes are set before capture (not a stream operation) */
     decode_mix_ctas_per_sm(m->dclass_max, m->mix_smem);
@@ -271,6 +382,11 @@ int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const i
             p.work = m->d_work + ncodes;
             p.msg = m->d_msg;
             p.msg_stride = mix_slab;
+            if (learned) {
+                p.learn = m->d_learn;
+                p.learn_class = m->d_learn_cls;
+                p.learn_iters = m->d_learn_iters;
+            }
             e = cudaMemsetAsync(p.work, 0, sizeof(unsigned), m->capture);
             if (e == cudaSuccess)
                 e = launch_decode_mix(p, m->dclass_max, m->mix_smem, mix_grid, m->capture);
@@ -298,6 +414,12 @@ int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const i
                 p.work = m->d_work + c;
                 p.msg = (char*)m->d_msg + side_off[code_side[c]];
                 p.msg_stride = code_slab[c];
+                if (learned) {
+                    p.learn = h->learn;
+                    p.learn_class = (const int8_t*)((const char*)h->learn +
+                                                    sizeof(uint32_t) * kLearnMaxIters * kLearnClasses);
+                    p.learn_iters = h->learn_iters;
+                }
                 e = cudaMemsetAsync(p.work, 0, sizeof(unsigned), s);
                 if (e == cudaSuccess)
                     e = pair_runs(h) ? launch_decode_pair(p, h->pair_kid, h->pair_smem, code_grid[c], s)
@@ -308,6 +430,34 @@ int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const i
                     e = cudaEventRecord(m->join[s], m->side[s]);
                 if (e == cudaSuccess)
                     e = cudaStreamWaitEvent(m->capture, m->join[s], 0);
+            }
+        }
+        if (learned && e == cudaSuccess) {
+            /* fallback: the failing rows, in processing order, through the plain one-launch kernel */
+            int* cnt = (int*)(m->d_fb_rows + nframes);
+            k_compact_failing<<<1, kCompactThreads, 0, m->capture>>>(m->d_order, ok, nframes, m->d_fb_rows, cnt,
+                                                                     fallback);
+            e = cudaGetLastError();
+            if (e == cudaSuccess && plain_max_iter > 0) {
+                MixParams p{};
+                p.codes = m->d_codes;
+                p.frame_code = m->d_frame_code;
+                p.order = m->d_fb_rows;
+                p.llr = llr;
+                p.llr_stride = llr_stride;
+                p.out = out;
+                p.out_stride = out_stride;
+                p.iters = iters;
+                p.ok = ok;
+                p.nframes = nframes;
+                p.nframes_dev = cnt;
+                p.max_iter = plain_max_iter;
+                p.work = m->d_work + ncodes;
+                p.msg = m->d_msg;
+                p.msg_stride = mix_slab;
+                e = cudaMemsetAsync(p.work, 0, sizeof(unsigned), m->capture);
+                if (e == cudaSuccess)
+                    e = launch_decode_mix(p, m->dclass_max, m->mix_smem, mix_grid, m->capture);
             }
         }
         const cudaError_t e2 = cudaStreamEndCapture(m->capture, &g);
@@ -323,6 +473,34 @@ int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const i
         }
     }
     return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* llr, size_t llr_stride,
+                      uint8_t* out, size_t out_stride, int32_t* iters, uint8_t* ok, int max_iter)
+{
+    return plan_mix(m, nframes, code, llr, llr_stride, out, out_stride, iters, ok, max_iter, false, 0, nullptr);
+}
+
+int drx_ldpc_mix_plan_learned(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* llr,
+                              size_t llr_stride, uint8_t* out, size_t out_stride, int32_t* iters, uint8_t* ok,
+                              uint8_t* fallback, int learned_iters, int plain_max_iter)
+{
+    return plan_mix(m, nframes, code, llr, llr_stride, out, out_stride, iters, ok, learned_iters, true,
+                    plain_max_iter, fallback);
+}
+
+int drx_ldpc_mix_set_learned(drx_ldpc_mix* m, int code_index, int iters, int nclass, const int8_t* class_of_degree,
+                             const float* scale, const float* offset)
+{
+    if (!m || code_index < 0 || code_index >= (int)m->codes.size()) {
+        set_error("drx_ldpc_mix_set_learned: code index out of range");
+        return -1;
+    }
+    return drx_ldpc_set_learned(m->codes[code_index], iters, nclass, class_of_degree, scale, offset);
 }
 
 int drx_ldpc_mix_set_tiling(drx_ldpc_mix* m, int tiling)

@@ -165,6 +165,23 @@ void drx_ldpc_mix_free(drx_ldpc_mix* m);
 int drx_ldpc_mix_plan(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* llr, size_t llr_stride,
                       uint8_t* out, size_t out_stride, int32_t* iters, uint8_t* ok, int max_iter);
 
+/* No counterpart in the reference.  The learned table of code index
+ * code_index (drx_ldpc_set_learned on that code's handle). */
+int drx_ldpc_mix_set_learned(drx_ldpc_mix* m, int code_index, int iters, int nclass, const int8_t* class_of_degree,
+                             const float* scale, const float* offset);
+
+/* No counterpart in the reference.  As drx_ldpc_mix_plan, for the learned
+ * decode with the plain decoder as fallback: every frame runs its code's
+ * learned table (at most learned_iters iterations, in the planned tiling);
+ * the rows whose syndrome still fails are then gathered on the device, in
+ * processing order, and decoded again from their LLRs by the plain decoder
+ * in one launch (at most plain_max_iter iterations; none if <= 0), all in
+ * the same CUDA graph.  fallback (device, nframes bytes, or NULL): 1 for
+ * the re-decoded rows.  Every code of the batch needs a learned table. */
+int drx_ldpc_mix_plan_learned(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* llr,
+                              size_t llr_stride, uint8_t* out, size_t out_stride, int32_t* iters, uint8_t* ok,
+                              uint8_t* fallback, int learned_iters, int plain_max_iter);
+
 /* Tilings of a mixed batch (identical results): one persistent launch over
  * all frames, one frame per CTA; or one persistent launch per code with the
  * code's own kernel (two frames per CTA where the frame-pair kernel

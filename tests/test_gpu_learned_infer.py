@@ -107,3 +107,30 @@ def test_set_learned_errors():
     dec.set_learned(None, None, None)
     with pytest.raises(RuntimeError):
         dec.decode_learned(llr, 5)
+
+
+def test_trained_table_gains_over_plain():
+    """The committed 12-iteration table for normal 3/5 8PSK (trained on the
+    GPU by the project's own forward/backward kernels) against the plain
+    decoder at the same 12-iteration budget on the same frames: at least
+    halves the frame error rate in the waterfall and needs fewer iterations;
+    with the plain fallback (30 iterations) nothing is lost."""
+    from dvbrx_b200 import train
+
+    table = train.load_table(0, "3_5", "8PSK", 12)
+    assert table is not None
+    dec = D.Ldpc(D.fec_lookup(0, "3_5"), "3_5")
+    train.apply_table(dec, table)
+    for es in (6.0, 6.25):
+        llr, info, _ = dec.generate(1024, es, seed=4242, constellation="8PSK", info=True)
+        pb, pi, po = dec.decode_device(llr, 12)
+        lb, li, lo, _ = dec.decode_learned(llr, 12, 0)
+        fb_bits, _, _, fb = dec.decode_learned(llr, 12, 30)
+        full, _, _ = dec.decode_device(llr, 30)
+        torch.cuda.synchronize()
+        fer_plain = float((pb != info).any(dim=1).float().mean())
+        fer_learned = float((lb != info).any(dim=1).float().mean())
+        assert fer_plain > 0.01, (es, fer_plain)
+        assert fer_learned <= 0.5 * fer_plain, (es, fer_learned, fer_plain)
+        assert float(li.float().mean()) < float(pi.float().mean()), es
+        assert int(((fb_bits != info).any(dim=1)).sum()) <= int(((full != info).any(dim=1)).sum()), es

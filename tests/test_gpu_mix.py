@@ -92,3 +92,54 @@ def test_mixed_batch_tilings_and_tuner():
         assert (out.cpu().numpy()[rows, : h.nbytes] == rb).all()
         assert (it.cpu().numpy()[rows] == ri).all()
     mix.close()
+
+
+def test_mixed_batch_learned_with_fallback():
+    """drx_ldpc_mix_plan_learned: every row equals its code's own learned
+    decode with fallback (drx_ldpc_decode_learned_device), in both tilings."""
+    import torch
+
+    from dvbrx_b200 import learned as Lm
+
+    n = 500
+    code, llr, handles = make_batch(n, 5)
+    mix = D.LdpcMix([(s, r) for s, r, _, _ in CODES])
+    L = 8
+    for c, (short, rate, _, _) in enumerate(CODES):
+        degs, cod = Lm.degree_classes(short, rate)
+        rng = np.random.default_rng(c)
+        scale = rng.uniform(0.8, 1.0, size=(L, len(degs)))
+        offset = rng.uniform(0.0, 1.0, size=(L, len(degs)))
+        mix.set_learned(c, scale, offset, cod)
+        handles[c].set_learned(scale, offset, cod)
+    out = torch.zeros((n, 7290), dtype=torch.uint8, device="cuda")
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    fb = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    mix.plan_learned(code, llr, out, it, ok, fb, L, 30)
+
+    want = {}
+    for c, h in enumerate(handles):
+        rows = np.nonzero(code == c)[0]
+        if not len(rows):
+            continue
+        sub = llr[torch.from_numpy(rows).cuda().long(), : h.N].contiguous()
+        b, i, o, f = h.decode_learned(sub, L, 30)
+        torch.cuda.synchronize()
+        want[c] = (rows, b.cpu().numpy(), i.cpu().numpy(), o.cpu().numpy(), f.cpu().numpy())
+    nfb = sum(int(w[4].sum()) for w in want.values())
+    assert 0 < nfb < n, "the batch should mix learned successes and fallbacks"
+    for tiling in (D.TILING_ONE_LAUNCH, D.TILING_PER_CODE):
+        out.zero_()
+        it.fill_(-1)
+        fb.fill_(7)
+        mix.set_tiling(tiling)
+        mix.run()
+        torch.cuda.synchronize()
+        got_b, got_i, got_o, got_f = out.cpu().numpy(), it.cpu().numpy(), ok.cpu().numpy(), fb.cpu().numpy()
+        for c, (rows, b, i, o, f) in want.items():
+            nb = handles[c].nbytes
+            assert (got_b[rows, :nb] == b).all(), (CODES[c], tiling)
+            assert (got_i[rows] == i).all(), (CODES[c], tiling)
+            assert (got_o[rows] == o).all(), (CODES[c], tiling)
+            assert (got_f[rows] == f).all(), (CODES[c], tiling)

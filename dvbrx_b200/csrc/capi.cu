@@ -195,6 +195,8 @@ struct Extra {
     int learn_iters = 0;
     const int32_t* rows = nullptr;
     const int* nframes_dev = nullptr;
+    unsigned* work = nullptr; /* frame counter (default: the handle's) */
+    void* msg = nullptr;      /* message scratch of the caller's, large enough (default: the handle's) */
 };
 
 /* Queue one decode of nframes device-resident frames. */
@@ -241,26 +243,27 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
         p.rows = x->rows;
         p.nframes_dev = x->nframes_dev;
     }
+    unsigned* work = x && x->work ? x->work : d->work;
     int grid;
     if (stop == 0 && use_pair(d)) {
         /* two frames per CTA */
         grid = std::min((nframes + 1) / 2, d->pair_ctas_per_sm * d->sms);
         p.group = 0;
-        p.work = d->work;
-        if (!cuda_ok(cudaMemsetAsync(d->work, 0, sizeof(unsigned), s), "cudaMemsetAsync"))
+        p.work = work;
+        if (!cuda_ok(cudaMemsetAsync(work, 0, sizeof(unsigned), s), "cudaMemsetAsync"))
             return -1;
         const size_t slab = decode_pair_msg_bytes(d->code.R);
-        if (!ensure_scratch(d, slab * (size_t)grid))
+        if (!(x && x->msg) && !ensure_scratch(d, slab * (size_t)grid))
             return -1;
-        p.msg = d->msg;
+        p.msg = x && x->msg ? x->msg : d->msg;
         p.msg_stride = slab;
         return cuda_ok(launch_decode_pair(p, d->pair_kid, d->pair_smem, grid, s), "decoder launch") ? 0 : -1;
     }
     if (stop == 0) {
         grid = std::min(nframes, capacity);
         p.group = 0;
-        p.work = d->work;
-        if (!cuda_ok(cudaMemsetAsync(d->work, 0, sizeof(unsigned), s), "cudaMemsetAsync"))
+        p.work = work;
+        if (!cuda_ok(cudaMemsetAsync(work, 0, sizeof(unsigned), s), "cudaMemsetAsync"))
             return -1;
     } else {
         const int G = stop;
@@ -281,9 +284,9 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
         p.nteams = nteams;
         p.team_sync = d->sync;
     }
-    if (!ensure_msg(d, grid))
+    if (!(x && x->msg) && !ensure_msg(d, grid))
         return -1;
-    p.msg = d->msg;
+    p.msg = x && x->msg ? x->msg : d->msg;
     p.msg_stride = decode_msg_bytes(d->code.R, d->code.dclass);
     return cuda_ok(launch_decode(p, d->code.dclass, d->smem, grid, s), "decoder launch") ? 0 : -1;
 }
@@ -300,6 +303,102 @@ __global__ void k_fallback_rows(const uint8_t* __restrict__ ok, int n, int32_t* 
         if (fail)
             rows[atomicAdd(count, 1)] = f;
     }
+}
+
+/* Streams, events, frame counters of the pipelined host call. */
+bool ensure_pipe(drx_ldpc* d)
+{
+    if (d->copy)
+        return true;
+    bool ok = cuda_ok(cudaStreamCreateWithFlags(&d->pipe[0], cudaStreamNonBlocking), "cudaStreamCreate") &&
+              cuda_ok(cudaStreamCreateWithFlags(&d->pipe[1], cudaStreamNonBlocking), "cudaStreamCreate") &&
+              cuda_ok(cudaMalloc(&d->chunk_work, 16 * sizeof(unsigned)), "cudaMalloc");
+    for (int k = 0; ok && k < 16; k++)
+        ok = cuda_ok(cudaEventCreateWithFlags(&d->chunk_ev[k], cudaEventDisableTiming), "cudaEventCreate");
+    if (ok)
+        ok = cuda_ok(cudaStreamCreateWithFlags(&d->copy, cudaStreamNonBlocking), "cudaStreamCreate");
+    return ok;
+}
+
+/* Message scratch of the largest per-frame launch of this handle. */
+size_t launch_msg_bytes(const drx_ldpc* d)
+{
+    size_t a = decode_msg_bytes(d->code.R, d->code.dclass) * (size_t)(d->ctas_per_sm * d->sms);
+    if (d->pair_ctas_per_sm > 0)
+        a = std::max(a, decode_pair_msg_bytes(d->code.R) * (size_t)(d->pair_ctas_per_sm * d->sms));
+    return a;
+}
+
+bool ensure_msg2(drx_ldpc* d, size_t need)
+{
+    if (d->msg2_cap >= need)
+        return true;
+    cudaFree(d->msg2);
+    d->msg2 = nullptr;
+    d->msg2_cap = 0;
+    if (!cuda_ok(cudaMalloc(&d->msg2, need), "cudaMalloc(messages)"))
+        return false;
+    d->msg2_cap = need;
+    return true;
+}
+
+/* Per-frame stopping on host rows, pipelined: the batch is cut into chunks;
+ * chunk c is copied into pinned memory, sent to the device on the copy
+ * stream, and decoded on decode stream c % 2 once its copy is done (its own
+ * frame counter, the stream's own message slab), its results returned on
+ * the same stream.  Copies of later chunks overlap earlier decodes, and the
+ * CTAs of chunk c + 1 take the SMs that chunk c's tail leaves. */
+int decode_host_pipelined(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t* iters, uint8_t* ok, int nframes,
+                          int max_iter)
+{
+    const size_t N = d->code.N, nb = d->nbytes;
+    const size_t mb = launch_msg_bytes(d);
+    if (!ensure_stage(d, nframes) || !ensure_pipe(d) || !ensure_scratch(d, mb) || !ensure_msg2(d, mb))
+        return -1;
+    const int nch = std::min(8, nframes / 256);
+    const int per = ((nframes + nch - 1) / nch + 1) & ~1;
+    /* work queued on the handle's stream goes first (it may use the scratch) */
+    if (!cuda_ok(cudaEventRecord(d->chunk_ev[15], d->stream), "cudaEventRecord") ||
+        !cuda_ok(cudaStreamWaitEvent(d->copy, d->chunk_ev[15], 0), "cudaStreamWaitEvent") ||
+        !cuda_ok(cudaStreamWaitEvent(d->pipe[0], d->chunk_ev[15], 0), "cudaStreamWaitEvent") ||
+        !cuda_ok(cudaStreamWaitEvent(d->pipe[1], d->chunk_ev[15], 0), "cudaStreamWaitEvent"))
+        return -1;
+    int rc = 0;
+    int c = 0;
+    for (size_t f0 = 0; f0 < (size_t)nframes && rc == 0; f0 += per, c++) {
+        const int n = (int)std::min((size_t)per, (size_t)nframes - f0);
+        memcpy(d->h_llr + f0 * N, llr + f0 * N, (size_t)n * N);
+        cudaStream_t ks = d->pipe[c & 1];
+        Extra x;
+        x.work = d->chunk_work + c;
+        x.msg = (c & 1) ? d->msg2 : d->msg;
+        if (!cuda_ok(cudaMemcpyAsync(d->d_llr + f0 * N, d->h_llr + f0 * N, (size_t)n * N, cudaMemcpyHostToDevice,
+                                     d->copy),
+                     "cudaMemcpyAsync") ||
+            !cuda_ok(cudaEventRecord(d->chunk_ev[c], d->copy), "cudaEventRecord") ||
+            !cuda_ok(cudaStreamWaitEvent(ks, d->chunk_ev[c], 0), "cudaStreamWaitEvent") ||
+            enqueue(d, d->d_llr + f0 * N, N, d->d_out + f0 * nb, nb, d->d_it + f0, d->d_ok + f0, n, max_iter, 0, ks,
+                    &x) ||
+            !cuda_ok(cudaMemcpyAsync(d->h_out + f0 * nb, d->d_out + f0 * nb, (size_t)n * nb, cudaMemcpyDeviceToHost,
+                                     ks),
+                     "cudaMemcpyAsync") ||
+            !cuda_ok(cudaMemcpyAsync(d->h_it + f0, d->d_it + f0, (size_t)n * 4, cudaMemcpyDeviceToHost, ks),
+                     "cudaMemcpyAsync") ||
+            !cuda_ok(cudaMemcpyAsync(d->h_ok + f0, d->d_ok + f0, (size_t)n, cudaMemcpyDeviceToHost, ks),
+                     "cudaMemcpyAsync"))
+            rc = -1;
+    }
+    const bool s0 = cuda_ok(cudaStreamSynchronize(d->pipe[0]), "decode");
+    const bool s1 = cuda_ok(cudaStreamSynchronize(d->pipe[1]), "decode");
+    const bool s2 = cuda_ok(cudaStreamSynchronize(d->copy), "copy");
+    if (rc || !s0 || !s1 || !s2)
+        return -1;
+    memcpy(out, d->h_out, (size_t)nframes * nb);
+    if (iters)
+        memcpy(iters, d->h_it, (size_t)nframes * 4);
+    if (ok)
+        memcpy(ok, d->h_ok, (size_t)nframes);
+    return 0;
 }
 
 bool ensure_fallback(drx_ldpc* d, size_t nframes)
@@ -402,6 +501,20 @@ void drx_ldpc_free(drx_ldpc* d)
         cudaStreamSynchronize(d->stream);
     release_stage(d);
     cudaFree(d->msg);
+    cudaFree(d->msg2);
+    cudaFree(d->chunk_work);
+    for (int k = 0; k < 16; k++)
+        if (d->chunk_ev[k])
+            cudaEventDestroy(d->chunk_ev[k]);
+    for (int k = 0; k < 2; k++)
+        if (d->pipe[k]) {
+            cudaStreamSynchronize(d->pipe[k]);
+            cudaStreamDestroy(d->pipe[k]);
+        }
+    if (d->copy) {
+        cudaStreamSynchronize(d->copy);
+        cudaStreamDestroy(d->copy);
+    }
     cudaFree(d->fb_rows);
     cudaFree(d->fb_ok);
     cudaFree(d->learn);
@@ -595,6 +708,8 @@ int drx_ldpc_decode_host(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t* 
     }
     if (nframes <= 0)
         return 0;
+    if (stop == 0 && nframes >= 512)
+        return decode_host_pipelined(d, llr, out, iters, ok, nframes, max_iter);
     const size_t N = d->code.N, nb = d->nbytes;
     cudaStream_t s = d->stream;
     if (!ensure_stage(d, nframes))

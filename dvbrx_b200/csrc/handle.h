@@ -45,6 +45,14 @@ struct drx_ldpc {
     int32_t* fb_rows = nullptr;
     uint8_t* fb_ok = nullptr;
     size_t fb_cap = 0;
+    /* pipelined host calls: two decode streams, one copy stream, chunk
+     * events and frame counters, and a second message slab */
+    cudaStream_t pipe[2] = {nullptr, nullptr};
+    cudaStream_t copy = nullptr;
+    cudaEvent_t chunk_ev[16] = {};
+    unsigned* chunk_work = nullptr;
+    void* msg2 = nullptr;
+    size_t msg2_cap = 0;
     /* staging of the host-pointer calls */
     int8_t* h_llr = nullptr;
     uint8_t* h_out = nullptr;

@@ -205,3 +205,19 @@ def test_variant_auto_choice():
     assert hi.set_variant(D.VARIANT_AUTO) == D.VARIANT_FRAME
     with pytest.raises(ValueError):
         hi.set_variant(D.VARIANT_PAIR)
+
+
+@pytest.mark.parametrize("short,rate,n", [(1, "1_2", 1500), (0, "3_5", 777), (0, "9_10", 600)])
+def test_host_call_pipelined_matches_device(short, rate, n):
+    """drx_ldpc_decode_host with per-frame stopping on 512 frames or more runs
+    in chunks on two streams; it returns the device call's results exactly."""
+    import torch
+
+    d = handle(short, rate)
+    llr = awgn_frames(short, rate, n, 1.5 if short else (2.6 if rate == "3_5" else 6.6), seed=31)
+    bits, it, ok = d.decode_host(llr, 30)
+    tb, ti, to = d.decode_device(torch.from_numpy(llr).cuda(), 30)
+    torch.cuda.synchronize()
+    assert np.array_equal(bits, tb.cpu().numpy())
+    assert np.array_equal(it, ti.cpu().numpy())
+    assert np.array_equal(ok, to.cpu().numpy())

@@ -260,19 +260,56 @@ def run_reference(args):
 # GPU
 # ---------------------------------------------------------------------------
 
+# ---------------------------------------------------------------------------
+# ranks: one process per GPU, frames sharded by rank (weak scaling)
+# ---------------------------------------------------------------------------
+
+def rank_env():
+    """(world size, rank, local rank) from the torchrun environment."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def init_ranks(world, backend="nccl", timeout_s=120):
+    """Process group for world > 1 (a short timeout: ranks that wait for a
+    lost peer end with an error)."""
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+
+def rank_seed(rank, k):
+    """Seed of Es/N0 batch k on a rank: every rank decodes its own frames."""
+    return 1000003 * (rank + 1) + k
+
+
+def max_over_ranks(x, world, device):
+    """The largest x over all ranks (a timed region's milliseconds)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_gbps(world, frames_per_rank, kldpc, ms):
+    """Whole-job information throughput: every rank's frames over the
+    slowest rank's time."""
+    return world * frames_per_rank * kldpc / (ms * 1e-3) / 1e9
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
 
     import dvbrx_b200 as D
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = rank_env()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    init_ranks(world, "nccl")
 
     p = D.fec_lookup(SHORT, RATE)
     dec = D.Ldpc(p, RATE)
@@ -286,7 +323,7 @@ def run_b200(args):
     # inputs: one batch per Es/N0 point, resident in HBM
     llr, info = [], []
     for k, es in enumerate(ESN0[: args.batches]):
-        l, inf, _ = dec.generate(F, es, seed=1000003 * (rank + 1) + k, constellation=CONST, info=True)
+        l, inf, _ = dec.generate(F, es, seed=rank_seed(rank, k), constellation=CONST, info=True)
         llr.append(l)
         info.append(inf)
     outs = [torch.empty((F, dec.nbytes), dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
@@ -322,17 +359,13 @@ def run_b200(args):
         errs[k] = (outs[k] != info[(args.warmup + k) % len(info)]).any(dim=1).sum()
     clocks = sampler.stop()
     launch_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = ev[0][0].elapsed_time(ev[-1][1])
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(ev[0][0].elapsed_time(ev[-1][1]), world, "cuda")
 
     it_all = torch.stack(iters).to(torch.int64)
     iters_sum = int(it_all.sum().item())
     frames_rank = args.steps * F
     fer = float(errs.sum().item()) / frames_rank
-    value = world * frames_rank * kldpc / (total_ms * 1e-3) / 1e9
+    value = aggregate_gbps(world, frames_rank, kldpc, total_ms)
 
     # roofline of the decode kernel (one launch per step)
     edges = dec.info.edges
@@ -398,14 +431,10 @@ def run_b200(args):
                                ok=l_ok[k], fallback=l_fb[k])
             lev[k][1].record(stream)
         torch.cuda.synchronize()
-        l_ms = lev[0][0].elapsed_time(lev[-1][1])
-        t = torch.tensor([l_ms], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        l_ms = float(t.item())
+        l_ms = max_over_ranks(lev[0][0].elapsed_time(lev[-1][1]), world, "cuda")
         l_err = sum(int((outs[k] != info[(args.warmup + k) % len(info)]).any(dim=1).sum()) for k in range(args.steps))
         fb_all = torch.stack(l_fb).float()
-        lval = world * frames_rank * kldpc / (l_ms * 1e-3) / 1e9
+        lval = aggregate_gbps(world, frames_rank, kldpc, l_ms)
         learned = {
             "value": lval, "unit": UNIT, "vs_plain": lval / value, "fer": l_err / frames_rank, "plain_fer": fer,
             "fallback_frac": float(fb_all.mean()),
@@ -429,12 +458,8 @@ def run_b200(args):
         t0 = time.perf_counter()
         for k in range(args.e2e_steps):
             dec.decode_host(host[k % len(host)], MAX_ITER)
-        dt = time.perf_counter() - t0
-        tt = torch.tensor([dt], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dt = float(tt.item())
-        e2e = {"value": world * args.e2e_steps * F * kldpc / dt / 1e9, "unit": UNIT,
+        dt = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+        e2e = {"value": aggregate_gbps(world, args.e2e_steps * F, kldpc, dt * 1e3), "unit": UNIT,
                "h2d_bytes_per_step": F * dec.N,
                "d2h_bytes_per_step": F * (dec.nbytes + 4 + 1),
                "api": "drx_ldpc_decode_host (host rows in, host bits/iterations/flags out; wall clock)"}

@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--e2e-steps", type=int, default=7)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned decoder's line items")
+    ap.add_argument("--mix-frames", type=int, default=16384,
+                    help="frames of the mixed-MODCOD batch (0: skip that line item)")
     ap.add_argument("--variant", default="auto", choices=["auto", "frame"],
                     help="decoder kernel: automatic choice, or the one-frame kernel")
     ap.add_argument("--batches", type=int, default=len(ESN0),
@@ -301,6 +303,90 @@ def aggregate_gbps(world, frames_per_rank, kldpc, ms):
     return world * frames_per_rank * kldpc / (ms * 1e-3) / 1e9
 
 
+def run_mix(args, world, rank, learned=False):
+    """The mixed-MODCOD batch (80 % normal / 20 % short frames, the eleven
+    DVB-S2 rates, every MODCOD of the rate, Es/N0 = the MODCOD's QEF value
+    + 0.5 dB) as one planned device batch: the tuner's tiling, then timed
+    replays of the CUDA graph.  learned: the learned 12-iteration tables of
+    every code with the plain decoder as fallback (None if a table is
+    missing)."""
+    import numpy as np
+    import torch
+
+    import dvbrx_b200 as D
+    from dvbrx_b200 import modcods as MC
+    from dvbrx_b200 import train as T
+
+    n = args.mix_frames
+    spec = MC.mixed_batch(n, seed=4242 + rank)
+    codes = sorted(set((s, r) for s, r, _, _ in spec))
+    cidx = {c: k for k, c in enumerate(codes)}
+    code = np.array([cidx[(s, r)] for s, r, _, _ in spec], np.int32)
+    tables = {}
+    if learned:
+        for s, r in codes:
+            t = T.load_table(s, r, "QPSK", LEARNED_ITERS) or T.load_table(s, r, "8PSK", LEARNED_ITERS)
+            if t is None:
+                return None
+            tables[(s, r)] = t
+    handles = {c: D.Ldpc(D.fec_lookup(*c), c[1]) for c in codes}
+    maxb = max(h.nbytes for h in handles.values())
+    llr = torch.zeros((n, 64800), dtype=torch.int8, device="cuda")
+    info = torch.zeros((n, maxb), dtype=torch.uint8, device="cuda")
+    groups = {}
+    for f, (s, r, c, es) in enumerate(spec):
+        groups.setdefault((s, r, c, es), []).append(f)
+    for g, (key, rows) in enumerate(sorted(groups.items())):
+        s, r, c, es = key
+        h = handles[(s, r)]
+        l, inf, _ = h.generate(len(rows), es, seed=rank_seed(rank, 100 + g), constellation=c, const_rate=r,
+                               info=True)
+        rt = torch.tensor(rows, dtype=torch.long, device="cuda")
+        llr[rt, : h.N] = l
+        info[rt, : h.nbytes] = inf
+    out = torch.zeros((n, maxb), dtype=torch.uint8, device="cuda")
+    it = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ok = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    fb = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    mix = D.LdpcMix(codes)
+    if learned:
+        for k, c in enumerate(codes):
+            t = tables[c]
+            mix.set_learned(k, t["scale"], t["offset"], t["class_of_degree"])
+        mix.plan_learned(code, llr, out, it, ok, fb, LEARNED_ITERS, MAX_ITER)
+    else:
+        mix.plan(code, llr, out, it, ok, MAX_ITER)
+    choice, t_one, t_per = mix.tune()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    reps = 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        mix.run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / reps, world, "cuda")
+    bits = sum(handles[(s, r)].kldpc for s, r, _, _ in spec)
+    errs = 0
+    for c, h in handles.items():
+        rows = torch.from_numpy(np.nonzero(code == cidx[c])[0]).cuda()
+        errs += int((out[rows, : h.nbytes] != info[rows, : h.nbytes]).any(dim=1).sum())
+    res = {"value": aggregate_gbps(world, 1, bits, ms), "unit": UNIT, "frames_per_rank": n, "codes": len(codes),
+           "normal_share": float(np.mean([s == 0 for s, _, _, _ in spec])), "ms_per_batch": ms,
+           "tiling": {D.TILING_ONE_LAUNCH: "one launch", D.TILING_PER_CODE: "per code"}[choice],
+           "tune_ms": {"one_launch": t_one, "per_code": t_per}, "fer": errs / n,
+           "avg_iterations": float(it.float().mean()),
+           "esn0": "QEF (EN 302 307-1 Table 13, normal-frame values for both sizes) + 0.5 dB",
+           "max_iter": MAX_ITER}
+    if learned:
+        res.update({"learned_iters": LEARNED_ITERS, "fallback_frac": float(fb.float().mean())})
+    mix.close()
+    return res
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -447,6 +533,14 @@ def run_b200(args):
         }
         dec.set_learned(None, None, None)
 
+    # the mixed-MODCOD batch, plain and learned with fallback
+    mix_res = mix_learned = None
+    if args.mix_frames > 0:
+        mix_res = run_mix(args, world, rank)
+        if not args.no_learned:
+            mix_learned = run_mix(args, world, rank, learned=True)
+        torch.cuda.empty_cache()
+
     # end to end through the C ABI with host buffers (synchronous call)
     e2e = None
     if args.e2e_steps > 0:
@@ -488,6 +582,7 @@ def run_b200(args):
             "decoder": "plain layered offset min-sum (bit-exact to the reference)",
             "quality": {"fer": fer, "avg_iterations": iters_sum / frames_rank},
             "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "learned": learned,
+            "mixed_modcod": mix_res, "mixed_modcod_learned": mix_learned,
             "gpu_launches": args.steps,
         }
         print(json.dumps(line))

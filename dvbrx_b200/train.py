@@ -222,8 +222,42 @@ def main(argv=None):
     ap.add_argument("--plain-iters", type=int, default=30)
     ap.add_argument("--weights", default="uniform", choices=["uniform", "ramp", "last"])
     ap.add_argument("--val", type=float, nargs="*", default=None, help="validation Es/N0 points")
+    ap.add_argument("--all-s2", action="store_true",
+                    help="one table per DVB-S2 code (normal and short), trained on the rate's QPSK MODCOD over "
+                         "[QEF - 0.25, QEF + 0.75] dB, into --out-dir")
+    ap.add_argument("--out-dir", default=None)
     a = ap.parse_args(argv)
     log = lambda s: print(s, flush=True)
+    if a.all_s2:
+        from .modcods import RATES, qef_db
+        out_dir = a.out_dir or TABLES
+        os.makedirs(out_dir, exist_ok=True)
+        for short in (0, 1):
+            for rate in RATES:
+                if short and rate == "9_10":
+                    continue
+                q = qef_db("QPSK", rate)
+                es = [q - 0.25, q + 0.75]
+                t0 = time.time()
+                model, hist = train(short, rate, "QPSK", a.iters, a.batch, es[0], es[1], a.steps, a.lr, a.seed,
+                                    None, a.weights, [q, q + 0.25, q + 0.5])
+                ms = [h["ms"] for h in hist[1:]] or [hist[0]["ms"]]
+                meta = {"short": short, "rate": rate, "constellation": "QPSK", "es": es, "batch": a.batch,
+                        "steps": a.steps, "lr": a.lr, "seed": a.seed, "weights": a.weights,
+                        "validation": model.validation, "loss_first": hist[0]["loss"],
+                        "loss_last": float(np.mean([h["loss"] for h in hist[-10:]])),
+                        "train_ms_per_step": float(np.median(ms)),
+                        "train_frames_per_s": a.batch / (float(np.median(ms)) * 1e-3),
+                        "train_wall_s": time.time() - t0}
+                table = export(model, meta)
+                path = os.path.join(out_dir, os.path.basename(table_path(short, rate, "QPSK", a.iters)))
+                with open(path, "w") as f:
+                    json.dump(table, f, indent=1)
+                log(json.dumps({"table": os.path.basename(path), "wall_s": meta["train_wall_s"],
+                                "validation": model.validation}))
+                del model
+                torch.cuda.empty_cache()
+        return 0
     if a.eval:
         with open(a.eval) as f:
             table = json.load(f)

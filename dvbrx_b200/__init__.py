@@ -101,6 +101,13 @@ def lib():
         L.drx_ldpc_set_variant.restype = ip
         L.drx_ldpc_device_error.argtypes = [vp]
         L.drx_ldpc_device_error.restype = ip
+        L.drx_bch_new.argtypes = [ctypes.POINTER(FecParams)]
+        L.drx_bch_new.restype = vp
+        L.drx_bch_free.argtypes = [vp]
+        L.drx_bch_decode.argtypes = [vp, vp]
+        L.drx_bch_decode.restype = ip
+        L.drx_bch_decode_device.argtypes = [vp, vp, sz, vp, ip, vp]
+        L.drx_bch_decode_device.restype = ip
         L.drx_ldpc_mix_set_learned.argtypes = [vp, ip, ip, ip, vp, vp, vp]
         L.drx_ldpc_mix_set_learned.restype = ip
         L.drx_ldpc_mix_plan_learned.argtypes = [vp, ip, vp, vp, sz, vp, sz, vp, vp, vp, ip, ip]
@@ -301,6 +308,49 @@ class Ldpc:
         if r != 0:
             raise RuntimeError("drx_ldpc_decode_learned_device: " + last_error())
         return out, iters, ok, fallback
+
+
+class Bch:
+    """The BCH outer code of one FEC configuration (``drx_bch_new`` /
+    ``drx_bch_free``), decoded on the GPU."""
+
+    def __init__(self, params):
+        self._lib = lib()
+        self.params = FecParams(params.short_frame, params.nldpc, params.kldpc, params.kbch, params.t)
+        self.h = self._lib.drx_bch_new(ctypes.byref(self.params))
+        if not self.h:
+            raise RuntimeError("drx_bch_new: " + last_error())
+        self.nbytes = self.params.kldpc // 8
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.drx_bch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def decode(self, word):
+        """``drx_bch_decode`` on one packed codeword (numpy uint8, corrected in
+        place); returns the corrected bit count or -1."""
+        assert word.dtype == np.uint8 and word.flags.c_contiguous and word.size >= self.nbytes
+        return self._lib.drx_bch_decode(self.h, word.ctypes.data)
+
+    def decode_device(self, cw, result=None, stream=None):
+        """``drx_bch_decode_device`` on torch CUDA rows [n, >= nbytes] uint8
+        (in place); returns the int32 results [n]."""
+        import torch
+
+        assert cw.is_cuda and cw.dtype == torch.uint8 and cw.dim() == 2 and cw.stride(1) == 1
+        n = cw.shape[0]
+        if result is None:
+            result = torch.empty(n, dtype=torch.int32, device=cw.device)
+        s = stream if stream is not None else torch.cuda.current_stream(cw.device)
+        r = self._lib.drx_bch_decode_device(self.h, cw.data_ptr(), cw.stride(0), result.data_ptr(), n,
+                                            stream_handle(s))
+        if r != 0:
+            raise RuntimeError("drx_bch_decode_device: " + last_error())
+        return result
 
 
 TILING_ONE_LAUNCH, TILING_PER_CODE = 1, 2  # DRX_TILING_*

@@ -270,6 +270,32 @@ int drx_ldpc_decode_learned_device(drx_ldpc* d, const int8_t* llr, size_t llr_st
 int drx_ldpc_schedule(int short_frame, const char* rate, int* nsteps, int* deg_max, int32_t* check_step,
                       int32_t* links);
 
+/* ---- BCH outer code (reference libdvbrx/include/dvbrx/fec.h:27-37) ---------
+ *
+ * The DVB-S2 BCH decoder on the GPU, with the reference's results
+ * (libdvbrx/src/bch.c:106-290): fed by the LDPC decoder's hard bits (kldpc =
+ * nbch bits, MSB first; the first kbch bits are the BBFRAME). */
+typedef struct drx_bch drx_bch;
+
+/* Replaces drx_bch_new (fec.h:29, bch.c:106-172): the code of p (normal
+ * frames over GF(2^16), short over GF(2^14), t from p).  NULL on failure. */
+drx_bch* drx_bch_new(const drx_fec_params* p);
+
+/* Replaces drx_bch_free (fec.h:30, bch.c:174-181); NULL-safe. */
+void drx_bch_free(drx_bch* b);
+
+/* Replaces drx_bch_decode (fec.h:31-37, bch.c:189-290): decode one codeword
+ * in host memory in place.  Returns the number of corrected bits, or -1 if
+ * it is uncorrectable (left untouched).  Synchronous. */
+int drx_bch_decode(drx_bch* b, uint8_t* cw);
+
+/* No counterpart in the reference (its decoder takes one word per call).
+ * Decode nframes device-resident codewords in place (row f at cw + f *
+ * stride) asynchronously on `stream`, straight after the LDPC decode of the
+ * same rows: result[f] (device) receives what drx_bch_decode returns.
+ * Returns 0 if the work was queued. */
+int drx_bch_decode_device(drx_bch* b, uint8_t* cw, size_t stride, int32_t* result, int nframes, void* stream);
+
 /* Device error word of the handle: 0, or the code of a device-side fault
  * report (2: a group barrier timed out).  Cleared by the call. */
 int drx_ldpc_device_error(drx_ldpc* d);

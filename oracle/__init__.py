@@ -84,6 +84,8 @@ def load_orc():
         lib.orc_encode.argtypes = [vp, vp, vp]
         lib.orc_decode_frame_learned.argtypes = [vp, vp, vp, ip, vp, vp, ip, vp]
         lib.orc_decode_frame_learned.restype = ip
+        lib.orc_bch_encode.argtypes = [ip, ip, ip, ip, vp, vp]
+        lib.orc_bch_encode.restype = ip
         _orc = lib
     return _orc
 
@@ -142,6 +144,50 @@ def _ptr_array(rows):
     for i, r in enumerate(rows):
         arr[i] = r.ctypes.data
     return arr
+
+
+def bch_encode(short_frame, rate, msgs):
+    """DVB-S2 BCH codewords of packed kbch-bit messages [n, >= ceil(kbch/8)]:
+    [n, kldpc/8] packed, MSB first (the oracle's encoder, checked by the
+    reference's decoder finding no error)."""
+    p = fec_params(short_frame, rate)
+    lib = load_orc()
+    msgs = np.ascontiguousarray(msgs, dtype=np.uint8)
+    out = np.zeros((msgs.shape[0], p.kldpc // 8), np.uint8)
+    for f in range(msgs.shape[0]):
+        row = np.concatenate([msgs[f], np.zeros(8, np.uint8)])
+        if lib.orc_bch_encode(int(short_frame), p.t, p.kbch, p.kldpc, row.ctypes.data, out[f].ctypes.data) < 0:
+            raise ValueError(rate)
+    return out
+
+
+class RefBch:
+    """The reference's BCH decoder (bch.c) compiled from its sources."""
+
+    def __init__(self, short_frame, rate):
+        self.lib = load_ref()
+        if self.lib is None:
+            raise RuntimeError("reference build missing")
+        vp = ctypes.c_void_p
+        self.lib.ref_bch_new.restype = vp
+        self.lib.ref_bch_new.argtypes = [ctypes.POINTER(FecParams)]
+        self.lib.ref_bch_free.argtypes = [vp]
+        self.lib.ref_bch_decode.argtypes = [vp, vp]
+        self.lib.ref_bch_decode.restype = ctypes.c_int
+        self.params = fec_params(short_frame, rate)
+        self.h = self.lib.ref_bch_new(ctypes.byref(self.params))
+
+    def decode(self, words):
+        """In a copy: (corrected words, results)."""
+        w = np.ascontiguousarray(words, dtype=np.uint8).copy()
+        res = np.zeros(w.shape[0], np.int32)
+        for f in range(w.shape[0]):
+            res[f] = self.lib.ref_bch_decode(self.h, w[f].ctypes.data)
+        return w, res
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref_bch_free(self.h)
 
 
 def learned_words(scale, offset):

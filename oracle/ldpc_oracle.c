@@ -386,3 +386,80 @@ void orc_encode(const orc_code* d, const uint8_t* info, uint8_t* cw)
     for (int k = 1; k < d->R; k++)
         p[k] ^= p[k - 1];
 }
+
+/*
+ * DVB-S2 BCH encoder (EN 302 307-1 5.3.1), for building test codewords: the
+ * generator g(x) is the product of the minimal polynomials of alpha^(2i+1),
+ * i < t, over GF(2^16) (normal frames, primitive x^16+x^5+x^3+x^2+1) or
+ * GF(2^14) (short frames, x^14+x^5+x^3+x+1); the codeword is the kbch
+ * message bits followed by the nbch - kbch bits of m(x) x^(nbch-kbch) mod
+ * g(x), packed MSB first.  Checked by the reference's own decoder
+ * (bch.c:189-290) finding no error in every encoded word.
+ */
+static int bch_gpoly(int short_frame, int t, uint8_t* g)
+{
+    const int m = short_frame ? 14 : 16, q = (1 << m) - 1;
+    const unsigned prim = short_frame ? 0x402B : 0x1002D;
+    uint16_t* ex = malloc(sizeof(uint16_t) * 2 * q);
+    int* lg = malloc(sizeof(int) * (q + 1));
+    unsigned x = 1;
+    for (int i = 0; i < q; i++) {
+        ex[i] = ex[i + q] = (uint16_t)x;
+        lg[x] = i;
+        x <<= 1;
+        if (x >> m)
+            x ^= prim;
+    }
+    int dg = 0;
+    g[0] = 1;
+    for (int i = 1; i < 2 * t; i += 2) {
+        /* minimal polynomial of alpha^i: product of (x + alpha^e), e over i's cyclotomic coset */
+        uint16_t p[40] = { 1 };
+        int dp = 0, e = i % q;
+        do {
+            const uint16_t beta = ex[e];
+            for (int k = dp + 1; k > 0; k--)
+                p[k] = p[k - 1] ^ (p[k] && beta ? ex[lg[p[k]] + lg[beta]] : 0);
+            p[0] = p[0] && beta ? ex[lg[p[0]] + lg[beta]] : 0;
+            dp++;
+            e = (2 * e) % q;
+        } while (e != i % q);
+        uint8_t r[200] = { 0 };
+        for (int a = 0; a <= dg; a++)
+            if (g[a])
+                for (int b = 0; b <= dp; b++)
+                    r[a + b] ^= (uint8_t)(p[b] & 1);
+        dg += dp;
+        memcpy(g, r, dg + 1);
+    }
+    free(ex);
+    free(lg);
+    return dg;
+}
+
+int orc_bch_encode(int short_frame, int t, int kbch, int nbch, const uint8_t* msg, uint8_t* cw)
+{
+    uint8_t g[200];
+    const int W = bch_gpoly(short_frame, t, g);
+    if (W != nbch - kbch)
+        return -1;
+    uint8_t* rem = calloc(W + 1, 1); /* rem[k]: coefficient of x^k */
+    for (int b = 0; b < kbch; b++) {
+        const int bit = (msg[b >> 3] >> (7 - (b & 7))) & 1;
+        const int top = rem[W - 1] ^ bit;
+        for (int k = W - 1; k > 0; k--)
+            rem[k] = rem[k - 1] ^ (top & g[k]);
+        rem[0] = (uint8_t)(top & g[0]);
+    }
+    memset(cw, 0, (nbch + 7) / 8);
+    for (int b = 0; b < kbch; b++)
+        if ((msg[b >> 3] >> (7 - (b & 7))) & 1)
+            cw[b >> 3] |= (uint8_t)(0x80 >> (b & 7));
+    for (int k = 0; k < W; k++) { /* parity bits, highest degree first */
+        const int b = kbch + (W - 1 - k);
+        if (rem[k])
+            cw[b >> 3] |= (uint8_t)(0x80 >> (b & 7));
+    }
+    free(rem);
+    return W;
+}

@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--e2e-steps", type=int, default=7)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned decoder's line items")
+    ap.add_argument("--no-bch", action="store_true", help="skip the BCH line item")
     ap.add_argument("--mix-frames", type=int, default=16384,
                     help="frames of the mixed-MODCOD batch (0: skip that line item)")
     ap.add_argument("--variant", default="auto", choices=["auto", "frame"],
@@ -387,6 +388,52 @@ def run_mix(args, world, rank, learned=False):
     return res
 
 
+def run_bch(nframes, world, reps=5):
+    """The BCH outer code of the workload on the device: nframes random
+    BBFRAMEs encoded on the GPU, decoded clean (the receiver's common case,
+    the remainder check only) and with t errors per frame at distinct
+    positions (syndromes, Berlekamp-Massey and the Chien search for every
+    frame); CUDA-event time of the decode calls only."""
+    import torch
+
+    import dvbrx_b200 as D
+
+    p = D.fec_lookup(SHORT, RATE)
+    b = D.Bch(p)
+    nb, kb = p.kldpc // 8, p.kbch // 8
+    g = torch.Generator(device="cuda").manual_seed(11)
+    clean = torch.zeros((nframes, nb), dtype=torch.uint8, device="cuda")
+    clean[:, :kb] = torch.randint(0, 256, (nframes, kb), generator=g, device="cuda", dtype=torch.uint8)
+    b.encode_device(clean)
+    base = torch.randint(0, p.kldpc, (nframes, 1), generator=g, device="cuda")
+    pos = (base + torch.arange(p.t, device="cuda")[None, :] * (p.kldpc // p.t)) % p.kldpc
+    masks = torch.zeros((nframes, nb), dtype=torch.int32, device="cuda")
+    masks.scatter_add_(1, pos // 8, (1 << (7 - pos % 8)).to(torch.int32))
+    noisy = clean ^ masks.to(torch.uint8)
+    res = torch.empty(nframes, dtype=torch.int32, device="cuda")
+    work = torch.empty_like(clean)
+    out = {"frames_per_rank": nframes, "code": "DVB-S2 normal rate 3/5 BCH (nbch %d, kbch %d, t %d)" % (
+        p.kldpc, p.kbch, p.t), "unit": UNIT}
+    for name, src, want in (("no_error", clean, 0), ("t_errors", noisy, p.t)):
+        work.copy_(src)
+        b.decode_device(work, res)  # warm-up
+        ms = 0.0
+        ok = True
+        for _ in range(reps):
+            work.copy_(src)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            b.decode_device(work, res)
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            ok = ok and bool((res == want).all()) and bool(torch.equal(work, clean))
+        ms = max_over_ranks(ms / reps, world, "cuda")
+        out[name] = {"value": aggregate_gbps(world, nframes, p.kbch, ms), "ms_per_batch": ms, "all_corrected": ok}
+    b.close()
+    return out
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -533,6 +580,9 @@ def run_b200(args):
         }
         dec.set_learned(None, None, None)
 
+    # the BCH outer code behind the decoder
+    bch = None if args.no_bch else run_bch(F, world)
+
     # the mixed-MODCOD batch, plain and learned with fallback
     mix_res = mix_learned = None
     if args.mix_frames > 0:
@@ -582,7 +632,7 @@ def run_b200(args):
             "decoder": "plain layered offset min-sum (bit-exact to the reference)",
             "quality": {"fer": fer, "avg_iterations": iters_sum / frames_rank},
             "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "learned": learned,
-            "mixed_modcod": mix_res, "mixed_modcod_learned": mix_learned,
+            "mixed_modcod": mix_res, "mixed_modcod_learned": mix_learned, "bch": bch,
             "gpu_launches": args.steps,
         }
         print(json.dumps(line))

@@ -108,6 +108,8 @@ def lib():
         L.drx_bch_decode.restype = ip
         L.drx_bch_decode_device.argtypes = [vp, vp, sz, vp, ip, vp]
         L.drx_bch_decode_device.restype = ip
+        L.drx_bch_encode_device.argtypes = [vp, vp, sz, ip, vp]
+        L.drx_bch_encode_device.restype = ip
         L.drx_ldpc_mix_set_learned.argtypes = [vp, ip, ip, ip, vp, vp, vp]
         L.drx_ldpc_mix_set_learned.restype = ip
         L.drx_ldpc_mix_plan_learned.argtypes = [vp, ip, vp, vp, sz, vp, sz, vp, vp, vp, ip, ip]
@@ -335,6 +337,17 @@ class Bch:
         place); returns the corrected bit count or -1."""
         assert word.dtype == np.uint8 and word.flags.c_contiguous and word.size >= self.nbytes
         return self._lib.drx_bch_decode(self.h, word.ctypes.data)
+
+    def encode_device(self, cw, stream=None):
+        """``drx_bch_encode_device``: rows [n, >= nbytes] uint8 holding the
+        message in their first kbch bits get their parity bits, in place."""
+        import torch
+
+        assert cw.is_cuda and cw.dtype == torch.uint8 and cw.dim() == 2 and cw.stride(1) == 1
+        s = stream if stream is not None else torch.cuda.current_stream(cw.device)
+        if self._lib.drx_bch_encode_device(self.h, cw.data_ptr(), cw.stride(0), cw.shape[0], stream_handle(s)) != 0:
+            raise RuntimeError("drx_bch_encode_device: " + last_error())
+        return cw
 
     def decode_device(self, cw, result=None, stream=None):
         """``drx_bch_decode_device`` on torch CUDA rows [n, >= nbytes] uint8

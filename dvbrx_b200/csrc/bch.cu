@@ -162,6 +162,31 @@ __global__ void __launch_bounds__(kBchThreads) k_bch_remainder(BchBatch b)
     b.queue[atomicAdd(b.count, 1)] = f;
 }
 
+/* Systematic encoding in place: the kbch message bits of each row are
+ * followed by the W parity bits of m(x) x^W mod g(x), highest degree first
+ * (the remainder of the same table division over the message bytes). */
+__global__ void __launch_bounds__(kBchThreads) k_bch_encode(BchBatch b, int kbytes)
+{
+    __shared__ unsigned long long tab[4 * 256 * kBchWords];
+    for (int k = threadIdx.x; k < 4 * 256 * kBchWords; k += blockDim.x)
+        tab[k] = b.c.tab[k];
+    __syncthreads();
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.nframes)
+        return;
+    uint8_t* w = b.cw + (size_t)f * b.stride;
+    unsigned long long r0 = 0, r1 = 0, r2 = 0;
+    for (int i = 0; i < kbytes; i++) {
+        const unsigned long long* t0 = tab + ((uint32_t)(r0 >> 56) ^ w[i]) * kBchWords;
+        r0 = (r0 << 8 | r1 >> 56) ^ t0[0];
+        r1 = (r1 << 8 | r2 >> 56) ^ t0[1];
+        r2 = (r2 << 8) ^ t0[2];
+    }
+    const unsigned long long r[3] = { r0, r1, r2 };
+    for (int k = 0; k < b.c.W / 8; k++)
+        w[kbytes + k] = (uint8_t)(r[k / 8] >> (56 - 8 * (k % 8)));
+}
+
 __global__ void __launch_bounds__(kChienThreads) k_bch_chien(BchBatch b)
 {
     __shared__ int s_roots, s_pos[kBchMaxT + 1];
@@ -434,6 +459,24 @@ int drx_bch_decode_device(drx_bch* b, uint8_t* cw, size_t stride, int32_t* resul
         return -1;
     }
     return bch_enqueue(b, cw, stride, result, nframes, stream ? (cudaStream_t)stream : b->stream);
+}
+
+int drx_bch_encode_device(drx_bch* b, uint8_t* cw, size_t stride, int nframes, void* stream)
+{
+    if (!b || (nframes > 0 && !cw) || stride < (size_t)(b->nbch / 8) || b->kbch % 8) {
+        set_error("drx_bch_encode_device: bad arguments");
+        return -1;
+    }
+    if (nframes <= 0)
+        return 0;
+    BchBatch p{};
+    p.c = b->dev;
+    p.cw = cw;
+    p.stride = stride;
+    p.nframes = nframes;
+    k_bch_encode<<<(nframes + kBchThreads - 1) / kBchThreads, kBchThreads, 0,
+                   stream ? (cudaStream_t)stream : b->stream>>>(p, b->kbch / 8);
+    return cuda_check(cudaGetLastError(), "BCH encode") ? 0 : -1;
 }
 
 int drx_bch_decode(drx_bch* b, uint8_t* cw)

@@ -296,6 +296,11 @@ int drx_bch_decode(drx_bch* b, uint8_t* cw);
  * Returns 0 if the work was queued. */
 int drx_bch_decode_device(drx_bch* b, uint8_t* cw, size_t stride, int32_t* result, int nframes, void* stream);
 
+/* No counterpart in the reference (the transmitter side, for test and
+ * benchmark frames): encode nframes device rows in place, the kbch message
+ * bits of each row followed by its nbch - kbch parity bits.  Asynchronous. */
+int drx_bch_encode_device(drx_bch* b, uint8_t* cw, size_t stride, int nframes, void* stream);
+
 /* Device error word of the handle: 0, or the code of a device-side fault
  * report (2: a group barrier timed out).  Cleared by the call. */
 int drx_ldpc_device_error(drx_ldpc* d);

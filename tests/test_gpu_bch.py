@@ -72,3 +72,16 @@ def test_bch_after_ldpc_on_device():
     want_w, want_r = oracle.RefBch(short, rate).decode(host)
     assert np.array_equal(res.cpu().numpy(), want_r)
     assert np.array_equal(bits.cpu().numpy(), want_w)
+
+
+@pytest.mark.parametrize("short,rate", [(0, "1_4"), (0, "2_3"), (0, "9_10"), (1, "1_2"), (1, "8_9")])
+def test_bch_encoder_matches_oracle(short, rate):
+    p = D.fec_lookup(short, rate)
+    rng = np.random.default_rng(5)
+    msgs = np.packbits(rng.integers(0, 2, (16, p.kbch), dtype=np.uint8), axis=1)
+    want = oracle.bch_encode(short, rate, msgs)
+    dev = torch.zeros((16, p.kldpc // 8), dtype=torch.uint8, device="cuda")
+    dev[:, : msgs.shape[1]] = torch.from_numpy(msgs).cuda()
+    D.Bch(p).encode_device(dev)
+    torch.cuda.synchronize()
+    assert np.array_equal(dev.cpu().numpy(), want)

@@ -388,6 +388,39 @@ def run_mix(args, world, rank, learned=False):
     return res
 
 
+def run_demap(nframes, world, hbm_peak, reps=5):
+    """The soft demapper ahead of the decoder: nframes 8PSK PLFRAMEs of the
+    workload's MODCOD (random received symbols; the kernel's work does not
+    depend on them) to int8 LLRs; CUDA-event time of the call; an HBM-bound
+    kernel (8 bytes of symbol in, 3 LLR bytes out per symbol)."""
+    import torch
+
+    import dvbrx_b200 as D
+
+    m = D.Demapper(CONST, RATE, SHORT)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    sym = torch.randn((nframes, 2 * m.nsym), generator=g, device="cuda")
+    n0 = torch.full((nframes,), 0.25, device="cuda")
+    llr = torch.empty((nframes, m.nldpc), dtype=torch.int8, device="cuda")
+    m.run(sym, n0, llr)
+    ms = 0.0
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        m.run(sym, n0, llr)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms = max_over_ranks(ms / reps, world, "cuda")
+    nbytes = nframes * (8 * m.nsym + m.nldpc + 4)
+    m.close()
+    return {"frames_per_rank": nframes, "modcod": "%s %s %s" % (CONST, RATE, "short" if SHORT else "normal"),
+            "ms_per_batch": ms, "msym_per_s": world * nframes * m.nsym / ms / 1e3,
+            "roofline": {"bound": "hbm", "achieved": nbytes / ms / 1e6, "peak": hbm_peak,
+                         "frac": nbytes / ms / 1e6 / hbm_peak, "unit": "GB/s",
+                         "algorithmic_bytes_per_launch": nbytes}}
+
+
 def run_bch(nframes, world, reps=5):
     """The BCH outer code of the workload on the device: nframes random
     BBFRAMEs encoded on the GPU, decoded clean (the receiver's common case,
@@ -580,8 +613,9 @@ def run_b200(args):
         }
         dec.set_learned(None, None, None)
 
-    # the BCH outer code behind the decoder
+    # the BCH outer code behind the decoder, the demapper ahead of it
     bch = None if args.no_bch else run_bch(F, world)
+    demap = None if args.no_bch else run_demap(F, world, hbm_peak)
 
     # the mixed-MODCOD batch, plain and learned with fallback
     mix_res = mix_learned = None
@@ -632,7 +666,7 @@ def run_b200(args):
             "decoder": "plain layered offset min-sum (bit-exact to the reference)",
             "quality": {"fer": fer, "avg_iterations": iters_sum / frames_rank},
             "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "learned": learned,
-            "mixed_modcod": mix_res, "mixed_modcod_learned": mix_learned, "bch": bch,
+            "mixed_modcod": mix_res, "mixed_modcod_learned": mix_learned, "bch": bch, "demapper": demap,
             "gpu_launches": args.steps,
         }
         print(json.dumps(line))

@@ -101,6 +101,15 @@ def lib():
         L.drx_ldpc_set_variant.restype = ip
         L.drx_ldpc_device_error.argtypes = [vp]
         L.drx_ldpc_device_error.restype = ip
+        L.drx_demapper_new.argtypes = [cp, cp, ip]
+        L.drx_demapper_new.restype = vp
+        L.drx_demapper_free.argtypes = [vp]
+        L.drx_demapper_symbols.argtypes = [vp]
+        L.drx_demapper_symbols.restype = ip
+        L.drx_demapper_run.argtypes = [vp, vp, sz, vp, vp, sz, ip, vp]
+        L.drx_demapper_run.restype = ip
+        L.drx_demapper_frame.argtypes = [vp, vp, ctypes.c_float, vp]
+        L.drx_demapper_frame.restype = ip
         L.drx_bch_new.argtypes = [ctypes.POINTER(FecParams)]
         L.drx_bch_new.restype = vp
         L.drx_bch_free.argtypes = [vp]
@@ -310,6 +319,51 @@ class Ldpc:
         if r != 0:
             raise RuntimeError("drx_ldpc_decode_learned_device: " + last_error())
         return out, iters, ok, fallback
+
+
+class Demapper:
+    """The reference receiver's soft demapper on the GPU (``drx_demapper_*``)."""
+
+    def __init__(self, constellation, rate, short_frame=0):
+        self._lib = lib()
+        self.h = self._lib.drx_demapper_new(constellation.encode(), rate.encode(), int(short_frame))
+        if not self.h:
+            raise RuntimeError("drx_demapper_new: " + last_error())
+        self.nsym = self._lib.drx_demapper_symbols(self.h)
+        self.nldpc = 16200 if short_frame else 64800
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.drx_demapper_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def run(self, sym, n0, llr=None, stream=None):
+        """Device batch: sym float32 [n, >= 2 nsym] (I/Q interleaved), n0
+        float32 [n]; returns int8 LLRs [n, nldpc]."""
+        import torch
+
+        assert sym.is_cuda and sym.dtype == torch.float32 and sym.dim() == 2 and sym.stride(1) == 1
+        n = sym.shape[0]
+        if llr is None:
+            llr = torch.empty((n, self.nldpc), dtype=torch.int8, device=sym.device)
+        n0 = n0.contiguous()
+        s = stream if stream is not None else torch.cuda.current_stream(sym.device)
+        r = self._lib.drx_demapper_run(self.h, sym.data_ptr(), sym.stride(0), n0.data_ptr(), llr.data_ptr(),
+                                       llr.stride(0), n, stream_handle(s))
+        if r != 0:
+            raise RuntimeError("drx_demapper_run: " + last_error())
+        return llr
+
+    def frame(self, sym, n0):
+        """One host frame (numpy float32 [2 nsym]) -> int8 LLRs [nldpc]."""
+        sym = np.ascontiguousarray(sym, dtype=np.float32)
+        out = np.zeros(self.nldpc, np.int8)
+        if self._lib.drx_demapper_frame(self.h, sym.ctypes.data, ctypes.c_float(n0), out.ctypes.data) != 0:
+            raise RuntimeError("drx_demapper_frame: " + last_error())
+        return out
 
 
 class Bch:

@@ -1,0 +1,309 @@
+/*
+ * The soft demapper of the reference receiver on the GPU
+ * (libdvbrx/src/demap.c:491-533, drx_demap_frame): received symbols of a
+ * PLFRAME (complex, interleaved float I/Q, unit average energy) to the
+ * decoder's int8 LLRs in codeword order, ahead of the LDPC decoder on the
+ * same stream.
+ *
+ * Max-log LLRs on the reference's scale: for bit b of symbol j,
+ *     LLR = quantise(2/n0 * (min_{label bit b = 1} d - min_{bit b = 0} d)),
+ *     d = x (-2 re p) + (y (-2 im p) + |p|^2)   (two fused multiply-adds,
+ *         as the reference's vector paths form it, demap.c:318-330),
+ * quantise = clamp to +-127 then round half to even; bit b of symbol j goes
+ * to codeword position order[b] * nsym + j (the bit interleaver).  QPSK has
+ * no interleaver and the closed form LLR = 2/n0 * 4/sqrt(2) * component.
+ * Points are the standard's, normalised to unit average energy
+ * (demap.c:183-190).  The results equal the reference's builds with fused
+ * multiply-adds (AVX2, AVX-512); its SSE2 build rounds the two products
+ * separately and can differ by one unit on rare ties.
+ *
+ * Grid rows walk the frames, threads take four consecutive symbols (16-byte
+ * loads, 4-byte stores per bit column); the points and their constants are
+ * kernel parameters (constant bank).
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+
+#include "../../include/dvbrx_b200.h"
+#include "codes_gen.h"
+#include "handle.h"
+
+namespace drxg {
+
+struct DemapParams {
+    int bits, nsym, nldpc, qpsk;
+    int order[8];
+    float ar[256], ai[256], e[256]; /* -2 re, -2 im, |p|^2 */
+    const float* sym;
+    size_t sym_stride; /* floats per frame */
+    const float* n0;   /* per frame */
+    int8_t* llr;
+    size_t llr_stride;
+    int nframes;
+};
+
+__device__ __forceinline__ int8_t quantise8(float v)
+{
+    v = fminf(fmaxf(v, -127.0f), 127.0f);
+    return (int8_t)__float2int_rn(v);
+}
+
+/* LLRs of one symbol, label bit b in out[b] */
+template <int BITS>
+__device__ __forceinline__ void demap_symbol(const DemapParams& p, float x, float y, float k, int8_t* out)
+{
+    if (BITS == 2) {
+        const float kq = k * 4.0f * 0.70710678118654752f; /* demap.c:496-500 */
+        out[0] = quantise8(__fmul_rn(kq, x));
+        out[1] = quantise8(__fmul_rn(kq, y));
+        return;
+    }
+    float m0[BITS], m1[BITS];
+#pragma unroll
+    for (int b = 0; b < BITS; b++)
+        m0[b] = m1[b] = INFINITY;
+#pragma unroll 8
+    for (int q = 0; q < (1 << BITS); q++) {
+        const float d = fmaf(x, p.ar[q], fmaf(y, p.ai[q], p.e[q]));
+#pragma unroll
+        for (int b = 0; b < BITS; b++) {
+            if ((q >> (BITS - 1 - b)) & 1)
+                m1[b] = fminf(m1[b], d);
+            else
+                m0[b] = fminf(m0[b], d);
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < BITS; b++)
+        out[b] = quantise8(__fmul_rn(k, __fsub_rn(m1[b], m0[b])));
+}
+
+/* Codeword position of label bit b of symbol j: QPSK bits 2j, 2j + 1;
+ * otherwise the bit interleaver's column order[b] */
+template <int BITS>
+__device__ __forceinline__ int llr_pos(const DemapParams& p, int b, int j)
+{
+    return BITS == 2 ? 2 * j + b : p.order[b] * p.nsym + j;
+}
+
+/* Grid rows walk the frames (2/n0 once per block), threads take four
+ * consecutive symbols: two 16-byte loads, and per label bit one 4-byte
+ * store (eight bytes for QPSK) where the row layout allows it. */
+template <int BITS>
+__global__ void __launch_bounds__(256) k_demap(const __grid_constant__ DemapParams p)
+{
+    __shared__ float s_k;
+    const int ngroups = (p.nsym + 3) / 4;
+    for (int f = blockIdx.y; f < p.nframes; f += gridDim.y) {
+        if (threadIdx.x == 0)
+            s_k = 2.0f / p.n0[f];
+        __syncthreads();
+        const float k = s_k;
+        const float* sym = p.sym + (size_t)f * p.sym_stride;
+        int8_t* llr = p.llr + (size_t)f * p.llr_stride;
+        const bool vec = ((uintptr_t)sym & 15) == 0 && ((uintptr_t)llr & 7) == 0 && (p.nsym & 3) == 0;
+        for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+            const int j0 = 4 * g;
+            int8_t v[4][BITS];
+            if (vec) {
+                const float4 a = *(const float4*)(sym + 2 * (size_t)j0);
+                const float4 c = *(const float4*)(sym + 2 * (size_t)j0 + 4);
+                demap_symbol<BITS>(p, a.x, a.y, k, v[0]);
+                demap_symbol<BITS>(p, a.z, a.w, k, v[1]);
+                demap_symbol<BITS>(p, c.x, c.y, k, v[2]);
+                demap_symbol<BITS>(p, c.z, c.w, k, v[3]);
+                if (BITS == 2) {
+                    uint2 w;
+                    w.x = (uint32_t)(uint8_t)v[0][0] | (uint32_t)(uint8_t)v[0][1] << 8 |
+                          (uint32_t)(uint8_t)v[1][0] << 16 | (uint32_t)(uint8_t)v[1][1] << 24;
+                    w.y = (uint32_t)(uint8_t)v[2][0] | (uint32_t)(uint8_t)v[2][1] << 8 |
+                          (uint32_t)(uint8_t)v[3][0] << 16 | (uint32_t)(uint8_t)v[3][1] << 24;
+                    *(uint2*)(llr + 2 * (size_t)j0) = w;
+                } else {
+#pragma unroll
+                    for (int b = 0; b < BITS; b++) {
+                        const int pos = llr_pos<BITS>(p, b, j0);
+                        if (pos + 3 < p.nldpc)
+                            *(uint32_t*)(llr + pos) = (uint32_t)(uint8_t)v[0][b] | (uint32_t)(uint8_t)v[1][b] << 8 |
+                                                      (uint32_t)(uint8_t)v[2][b] << 16 |
+                                                      (uint32_t)(uint8_t)v[3][b] << 24;
+                        else
+                            for (int s = 0; s < 4; s++)
+                                if (pos + s < p.nldpc)
+                                    llr[pos + s] = v[s][b];
+                    }
+                }
+            } else {
+                for (int s = 0; s < 4; s++) {
+                    const int j = j0 + s;
+                    if (j >= p.nsym)
+                        break;
+                    demap_symbol<BITS>(p, sym[2 * (size_t)j], sym[2 * (size_t)j + 1], k, v[s]);
+#pragma unroll
+                    for (int b = 0; b < BITS; b++) {
+                        const int pos = llr_pos<BITS>(p, b, j);
+                        if (pos < p.nldpc)
+                            llr[pos] = v[s][b];
+                    }
+                }
+            }
+        }
+        __syncthreads(); /* s_k is rewritten for the next frame */
+    }
+}
+
+}  // namespace drxg
+
+using namespace drxg;
+
+struct drx_demapper {
+    int device = 0, sms = 0;
+    DemapParams p{};
+    cudaStream_t stream = nullptr;
+    float* d_sym = nullptr;
+    float* d_n0 = nullptr;
+    int8_t* d_llr = nullptr;
+};
+
+namespace {
+
+cudaError_t launch_demap(const DemapParams& p, int sms, cudaStream_t s)
+{
+    const int gx = (((p.nsym + 3) / 4) + 255) / 256;
+    const int gy = std::max(1, std::min(p.nframes, std::max(1, 8 * sms / gx)));
+    const dim3 grid(gx, std::min(gy, 65535));
+    switch (p.qpsk ? 2 : p.bits) {
+    case 2:
+        k_demap<2><<<grid, 256, 0, s>>>(p);
+        break;
+    case 3:
+        k_demap<3><<<grid, 256, 0, s>>>(p);
+        break;
+    case 4:
+        k_demap<4><<<grid, 256, 0, s>>>(p);
+        break;
+    case 5:
+        k_demap<5><<<grid, 256, 0, s>>>(p);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+drx_demapper* drx_demapper_new(const char* constellation, const char* rate, int short_frame)
+{
+    if (!constellation || !rate) {
+        set_error("drx_demapper_new: NULL argument");
+        return nullptr;
+    }
+    const cg_const* row = nullptr;
+    for (size_t i = 0; i < sizeof(cg_consts) / sizeof(*cg_consts); i++)
+        if (!strcmp(cg_consts[i].name, constellation) && !strcmp(cg_consts[i].rate, rate) &&
+            cg_consts[i].short_frame == (short_frame ? 1 : 0))
+            row = &cg_consts[i];
+    if (!row || (row->order[0] >= 0 && (row->bits < 3 || row->bits > 5))) {
+        set_error(std::string("drx_demapper_new: no DVB-S2 constellation ") + constellation + " " + rate);
+        return nullptr;
+    }
+    drx_demapper* m = new drx_demapper();
+    DemapParams& p = m->p;
+    p.bits = row->bits;
+    p.qpsk = row->order[0] < 0;
+    p.nldpc = short_frame ? 16200 : 64800;
+    p.nsym = (p.nldpc + p.bits - 1) / p.bits;
+    for (int b = 0; b < 8; b++)
+        p.order[b] = row->order[b] < 0 ? 0 : row->order[b];
+    const int np = 1 << row->bits;
+    double e = 0;
+    for (int i = 0; i < np; i++)
+        e += (double)row->points[2 * i] * row->points[2 * i] + (double)row->points[2 * i + 1] * row->points[2 * i + 1];
+    const float g = (float)(1.0 / sqrt(e / np));
+    for (int i = 0; i < np; i++) {
+        const float re = row->points[2 * i] * g, im = row->points[2 * i + 1] * g;
+        p.ar[i] = -2.0f * re;
+        p.ai[i] = -2.0f * im;
+        p.e[i] = fmaf(re, re, im * im);
+    }
+    if (!cuda_check(cudaGetDevice(&m->device), "cudaGetDevice") ||
+        !cuda_check(cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, m->device), "attribute") ||
+        !cuda_check(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate") ||
+        !cuda_check(cudaMalloc(&m->d_sym, sizeof(float) * 2 * (size_t)p.nsym), "cudaMalloc") ||
+        !cuda_check(cudaMalloc(&m->d_n0, sizeof(float)), "cudaMalloc") ||
+        !cuda_check(cudaMalloc(&m->d_llr, (size_t)p.nldpc), "cudaMalloc")) {
+        drx_demapper_free(m);
+        return nullptr;
+    }
+    return m;
+}
+
+void drx_demapper_free(drx_demapper* m)
+{
+    if (!m)
+        return;
+    if (m->stream)
+        cudaStreamSynchronize(m->stream);
+    cudaFree(m->d_sym);
+    cudaFree(m->d_n0);
+    cudaFree(m->d_llr);
+    if (m->stream)
+        cudaStreamDestroy(m->stream);
+    delete m;
+}
+
+int drx_demapper_symbols(const drx_demapper* m) { return m ? m->p.nsym : -1; }
+
+int drx_demapper_run(drx_demapper* m, const float* sym, size_t sym_stride, const float* n0, int8_t* llr,
+                     size_t llr_stride, int nframes, void* stream)
+{
+    if (!m || (nframes > 0 && (!sym || !n0 || !llr))) {
+        set_error("drx_demapper_run: NULL argument");
+        return -1;
+    }
+    if (sym_stride < 2 * (size_t)m->p.nsym || llr_stride < (size_t)m->p.nldpc || (sym_stride & 1) ||
+        ((uintptr_t)sym & 7)) {
+        set_error("drx_demapper_run: strides below the frame size or unaligned symbols");
+        return -1;
+    }
+    if (nframes <= 0)
+        return 0;
+    DemapParams p = m->p;
+    p.sym = sym;
+    p.sym_stride = sym_stride;
+    p.n0 = n0;
+    p.llr = llr;
+    p.llr_stride = llr_stride;
+    p.nframes = nframes;
+    return cuda_check(launch_demap(p, m->sms, stream ? (cudaStream_t)stream : m->stream), "demapper launch") ? 0
+                                                                                                                : -1;
+}
+
+int drx_demapper_frame(drx_demapper* m, const float* sym, float n0, int8_t* llr)
+{
+    if (!m || !sym || !llr) {
+        set_error("drx_demapper_frame: NULL argument");
+        return -1;
+    }
+    const size_t ns = 2 * (size_t)m->p.nsym;
+    if (!cuda_check(cudaMemcpyAsync(m->d_sym, sym, sizeof(float) * ns, cudaMemcpyHostToDevice, m->stream),
+                    "cudaMemcpyAsync") ||
+        !cuda_check(cudaMemcpyAsync(m->d_n0, &n0, sizeof(float), cudaMemcpyHostToDevice, m->stream),
+                    "cudaMemcpyAsync") ||
+        drx_demapper_run(m, m->d_sym, ns, m->d_n0, m->d_llr, (size_t)m->p.nldpc, 1, m->stream) ||
+        !cuda_check(cudaMemcpyAsync(llr, m->d_llr, (size_t)m->p.nldpc, cudaMemcpyDeviceToHost, m->stream),
+                    "cudaMemcpyAsync") ||
+        !cuda_check(cudaStreamSynchronize(m->stream), "demapper"))
+        return -1;
+    return 0;
+}
+
+}  // extern "C"

@@ -301,6 +301,35 @@ int drx_bch_decode_device(drx_bch* b, uint8_t* cw, size_t stride, int32_t* resul
  * bits of each row followed by its nbch - kbch parity bits.  Asynchronous. */
 int drx_bch_encode_device(drx_bch* b, uint8_t* cw, size_t stride, int nframes, void* stream);
 
+/* ---- soft demapper (reference libdvbrx/src/demap.c:491-533) -------------
+ *
+ * The reference receiver's max-log demapper on the GPU, ahead of the LDPC
+ * decoder: received symbols (interleaved float I/Q, unit average energy) to
+ * int8 LLRs in codeword order, 2/n0 x (min distance, bit 1 - min distance,
+ * bit 0) quantised as the reference does, the MODCOD's bit interleaver
+ * applied.  Results equal drx_demap_frame of the reference's builds with
+ * fused multiply-adds (AVX2, AVX-512).  DVB-S2 QPSK, 8PSK, 16APSK, 32APSK.
+ * Separate names from the reference's drx_demap_* (whose handle also serves
+ * its hard-decision and noise-estimation calls): no counterpart to replace. */
+typedef struct drx_demapper drx_demapper;
+
+/* A demapper for a MODCOD ("8PSK", "3_5", normal or short frames); NULL for
+ * an unknown one. */
+drx_demapper* drx_demapper_new(const char* constellation, const char* rate, int short_frame);
+void drx_demapper_free(drx_demapper* m);
+
+/* Symbols per frame (the reference's drx_demap_symbols). */
+int drx_demapper_symbols(const drx_demapper* m);
+
+/* nframes device frames: sym + f * sym_stride (floats, 8-byte aligned) holds
+ * frame f's symbols, n0[f] its noise variance per complex symbol (device);
+ * llr + f * llr_stride receives its nldpc LLRs.  Asynchronous on `stream`. */
+int drx_demapper_run(drx_demapper* m, const float* sym, size_t sym_stride, const float* n0, int8_t* llr,
+                     size_t llr_stride, int nframes, void* stream);
+
+/* One frame in host memory, synchronous (drx_demap_frame's arguments). */
+int drx_demapper_frame(drx_demapper* m, const float* sym, float n0, int8_t* llr);
+
 /* Device error word of the handle: 0, or the code of a device-side fault
  * report (2: a group barrier timed out).  Cleared by the call. */
 int drx_ldpc_device_error(drx_ldpc* d);

@@ -101,6 +101,10 @@ def lib():
         L.drx_ldpc_set_variant.restype = ip
         L.drx_ldpc_device_error.argtypes = [vp]
         L.drx_ldpc_device_error.restype = ip
+        L.drx_bb_descramble_device.argtypes = [vp, sz, ip, ip, vp]
+        L.drx_bb_descramble_device.restype = ip
+        L.drx_bbheader_check_device.argtypes = [vp, sz, vp, ip, vp]
+        L.drx_bbheader_check_device.restype = ip
         L.drx_demapper_new.argtypes = [cp, cp, ip]
         L.drx_demapper_new.restype = vp
         L.drx_demapper_free.argtypes = [vp]
@@ -319,6 +323,33 @@ class Ldpc:
         if r != 0:
             raise RuntimeError("drx_ldpc_decode_learned_device: " + last_error())
         return out, iters, ok, fallback
+
+
+def bb_descramble(frames, kbch_bytes, stream=None):
+    """``drx_bb_descramble_device`` on torch CUDA rows [n, >= kbch_bytes]
+    uint8, in place."""
+    import torch
+
+    assert frames.is_cuda and frames.dtype == torch.uint8 and frames.dim() == 2 and frames.stride(1) == 1
+    s = stream if stream is not None else torch.cuda.current_stream(frames.device)
+    if lib().drx_bb_descramble_device(frames.data_ptr(), frames.stride(0), int(kbch_bytes), frames.shape[0],
+                                      stream_handle(s)) != 0:
+        raise RuntimeError("drx_bb_descramble_device: " + last_error())
+    return frames
+
+
+def bbheader_check(frames, stream=None):
+    """``drx_bbheader_check_device``: int8 status per row (0 valid, 1 valid
+    in High Efficiency Mode, -1 invalid)."""
+    import torch
+
+    assert frames.is_cuda and frames.dtype == torch.uint8 and frames.dim() == 2 and frames.stride(1) == 1
+    st = torch.empty(frames.shape[0], dtype=torch.int8, device=frames.device)
+    s = stream if stream is not None else torch.cuda.current_stream(frames.device)
+    if lib().drx_bbheader_check_device(frames.data_ptr(), frames.stride(0), st.data_ptr(), frames.shape[0],
+                                       stream_handle(s)) != 0:
+        raise RuntimeError("drx_bbheader_check_device: " + last_error())
+    return st
 
 
 class Demapper:

@@ -330,6 +330,23 @@ int drx_demapper_run(drx_demapper* m, const float* sym, size_t sym_stride, const
 /* One frame in host memory, synchronous (drx_demap_frame's arguments). */
 int drx_demapper_frame(drx_demapper* m, const float* sym, float n0, int8_t* llr);
 
+/* ---- baseband layer (reference libdvbrx/src/bb.c:46-101) ----------------
+ *
+ * No counterpart with these arguments in the reference (its calls take one
+ * frame in host memory): device batches straight after the BCH decoder.
+ * Stream NULL is the legacy default stream. */
+
+/* Descramble nframes packed BBFRAMEs in place (frame f at frames + f *
+ * stride, kbch_bytes long, <= 7274): XOR with the BB scrambling sequence,
+ * as drx_bb_descramble (bb.c:62-67).  Asynchronous. */
+int drx_bb_descramble_device(uint8_t* frames, size_t stride, int kbch_bytes, int nframes, void* stream);
+
+/* Check the BBHEADER (first 10 bytes) of nframes descrambled frames:
+ * status[f] (device) = 0 if drx_bbheader_parse (bb.c:69-101) accepts it in
+ * normal mode, 1 if it accepts it in DVB-T2 High Efficiency Mode, -1 if it
+ * rejects it.  Asynchronous. */
+int drx_bbheader_check_device(const uint8_t* frames, size_t stride, int8_t* status, int nframes, void* stream);
+
 /* Device error word of the handle: 0, or the code of a device-side fault
  * report (2: a group barrier timed out).  Cleared by the call. */
 int drx_ldpc_device_error(drx_ldpc* d);

@@ -66,6 +66,17 @@ __device__ __forceinline__ uint32_t sadd(uint32_t a, uint32_t b)
  * (half-rate) ALU pipe to the min/max, select and permute work */
 __device__ __forceinline__ uint32_t neg2(uint32_t x) { return __vsub2(0u, x); }
 __device__ __forceinline__ uint32_t abs2(uint32_t x) { return __vmaxs2(x, neg2(x)); }
+/* 16-bit shared-memory accesses at a 32-bit shared address */
+__device__ __forceinline__ uint32_t lds16(uint32_t a)
+{
+    unsigned short v;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void sts16(uint32_t a, uint32_t v)
+{
+    asm volatile("st.shared.u16 [%0], %1;" ::"r"(a), "h"((unsigned short)v));
+}
 __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
 {
     return __heq2_mask(*(const __half2*)&a, *(const __half2*)&b);
@@ -91,14 +102,15 @@ template <int DM, bool EXACT>
 struct PairCheck {
     static constexpr int S = (DM + 1) / 2;
     int r;
-    int addr[S];
+    uint32_t addr[S]; /* shared-memory byte addresses of the owned links' posteriors */
     uint32_t x[S];
     uint32_t live, inm, outm; /* bit 2k: owned slot k is a link / is read late / is written early */
     uint32_t n0, n1, p0, p1, idxh, sgn;
     uint32_t min0, min1, sg, mn0, mn1;
 
     __device__ __forceinline__ void setup(const int2* __restrict__ ent, int cnt, int K, int q, int i, int j,
-                                          int rr, uint2 rec, uint32_t fresh, unsigned long long meta)
+                                          int rr, uint2 rec, uint32_t fresh, unsigned long long meta,
+                                          uint32_t sbase)
     {
         r = rr;
         const int D = EXACT ? DM : cnt + 2;
@@ -121,7 +133,7 @@ struct PairCheck {
                 const int2 e = ent[min(c, D - 1) - 2];
                 a = e.x + j + (j < e.y ? kQCp : 0);
             }
-            addr[k] = a;
+            addr[k] = sbase + 2u * (uint32_t)a;
         }
         /* messages: zero for a lane in its first iteration */
         const uint32_t w0 = rec.x & ~fresh;
@@ -140,7 +152,7 @@ struct PairCheck {
     /* extrinsic input of owned slot k: posterior minus the old message */
     __device__ __forceinline__ uint32_t extrinsic(const uint16_t* __restrict__ post, int k) const
     {
-        const uint32_t v = sx2(post[addr[k]]);
+        const uint32_t v = sx2(lds16(addr[k]));
         const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(2 * k) * 0x00010001u);
         const uint32_t sm = lmask(sgn << (15 - 2 * k));
         return sadd(v, sel(sm, sel(im, n1, n0), sel(im, p1, p0)));
@@ -218,7 +230,7 @@ struct PairCheck {
         for (int k = 0; k < S; k++)
             if ((outm >> (2 * k)) & 1u) {
                 uint32_t above, neg;
-                post[addr[k]] = (uint16_t)update(k, above, neg);
+                sts16(addr[k], update(k, above, neg));
             }
     }
 
@@ -234,7 +246,7 @@ struct PairCheck {
             uint32_t above, neg;
             const uint32_t nv = update(k, above, neg);
             if ((wm >> (2 * k)) & 1u)
-                post[addr[k]] = (uint16_t)nv;
+                sts16(addr[k], nv);
             nidx = sel(above, nidx, (uint32_t)(2 * k + 1) * 0x00010001u);
             nsg |= neg & (0x00010001u << (2 * k));
         }
@@ -388,7 +400,8 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
     };
     PairCheck<DM, EXACT> ck;
     if (active) {
-        ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, t & 1, rec, fresh, meta);
+        ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, t & 1, rec, fresh, meta,
+                 (uint32_t)__cvta_generic_to_shared(fr.post));
         ck.read_all(fr.post);
     }
     if (nlev > 1) {

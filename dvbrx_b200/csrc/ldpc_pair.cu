@@ -131,7 +131,8 @@ struct PairCheck {
             } else {
                 /* a slot past the degree takes the last link's address: read, never used */
                 const int2 e = ent[min(c, D - 1) - 2];
-                a = e.x + j + (j < e.y ? kQCp : 0);
+                addr[k] = (uint32_t)e.x + 2u * (uint32_t)j + (j < e.y ? 2u * kQCp : 0u);
+                continue;
             }
             addr[k] = sbase + 2u * (uint32_t)a;
         }
@@ -166,17 +167,32 @@ struct PairCheck {
         sg ^= v;
     }
 
-    /* every owned slot but the late ones, without branches */
+    /* every owned slot but the late ones, without branches; minimums folded
+     * two slots at a time: min1 = second smallest of {min0, min1, a, b} =
+     * min3(max(min0, min(a, b)), min1, max(a, b)).  LEV: the layer has late
+     * slots; otherwise only the slots that can be absent are masked (the
+     * previous parity of check (0, 0), the odd slot past the degree). */
+    template <bool LEV>
     __device__ __forceinline__ void read_all(const uint16_t* __restrict__ post)
     {
-        const uint32_t excl = ~live | inm;
+        const uint32_t excl = LEV ? (~live | inm) : ~live;
 #pragma unroll
         for (int k = 0; k < S; k++) {
             uint32_t v = extrinsic(post, k);
-            v = ((excl >> (2 * k)) & 1u) ? 0x00FF00FFu : v;
+            if (LEV || !EXACT || k == 0 || (k == S - 1 && (DM & 1)))
+                v = ((excl >> (2 * k)) & 1u) ? 0x00FF00FFu : v;
             x[k] = v;
-            fold(v);
         }
+#pragma unroll
+        for (int k = 0; k + 1 < S; k += 2) {
+            const uint32_t a = abs2(x[k]), b = abs2(x[k + 1]);
+            const uint32_t lo = __vmins2(a, b), hi = __vmaxs2(a, b);
+            min1 = __vimin3_s16x2(__vmaxs2(min0, lo), min1, hi);
+            min0 = __vimin3_s16x2(min0, a, b);
+            sg ^= x[k] ^ x[k + 1];
+        }
+        if (S & 1)
+            fold(x[S - 1]);
     }
 
     /* the late slots (their bits were written by earlier levels) */
@@ -265,7 +281,7 @@ struct PairCheck {
 
 struct PairFrame {
     uint16_t* post;
-    const int2* ent;
+    const int2* ent; /* (shared byte address of the link for check 0 before the wrap, a) */
     const uint16_t* eoff;
     const uint32_t* steps;
 };
@@ -282,8 +298,13 @@ __device__ PairFrame stage_pair(const DevCode& c, char* smem)
     uint16_t* eoff = (uint16_t*)(smem + off);
     off += a16p(sizeof(uint16_t) * (c.q + 1));
     uint32_t* steps = (uint32_t*)(smem + off);
-    for (int k = threadIdx.x; k < c.nent; k += blockDim.x)
-        ent[k] = c.ent[k];
+    /* entries as shared byte addresses: x = posterior address of link (g, a)
+     * for check 0, before the wrap (link of check j: x + 2 j, + 720 if j < a) */
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(f.post);
+    for (int k = threadIdx.x; k < c.nent; k += blockDim.x) {
+        const int2 e = c.ent[k];
+        ent[k] = make_int2((int)(sbase + 2u * (uint32_t)e.x), e.y);
+    }
     for (int k = threadIdx.x; k <= c.q; k += blockDim.x)
         eoff[k] = c.eoff[k];
     for (int k = threadIdx.x; k < c.nsteps; k += blockDim.x)
@@ -353,7 +374,7 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
             const int e1 = fr.eoff[i + 1];
             for (int e = fr.eoff[i]; e < e1; e++) {
                 const int2 en = fr.ent[e];
-                const uint32_t v = sx2(post[en.x + j + (j < en.y ? kQCp : 0)]);
+                const uint32_t v = sx2(lds16((uint32_t)en.x + 2u * (uint32_t)j + (j < en.y ? 2u * kQCp : 0u)));
                 par ^= v;
                 z |= __vsub2(v, 0x00010001u) & ~v;
             }
@@ -402,7 +423,10 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
     if (active) {
         ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, t & 1, rec, fresh, meta,
                  (uint32_t)__cvta_generic_to_shared(fr.post));
-        ck.read_all(fr.post);
+        if (nlev > 1)
+            ck.template read_all<true>(fr.post);
+        else
+            ck.template read_all<false>(fr.post);
     }
     if (nlev > 1) {
         const int lev = (int)(meta & 0xFF);

@@ -198,13 +198,16 @@ struct PairCheck {
     /* the late slots (their bits were written by earlier levels) */
     __device__ __forceinline__ void read_late(const uint16_t* __restrict__ post)
     {
+        uint32_t v[S];
 #pragma unroll
         for (int k = 0; k < S; k++)
-            if ((inm >> (2 * k)) & 1u) {
-                const uint32_t v = extrinsic(post, k);
-                x[k] = v;
-                fold(v);
-            }
+            v[k] = extrinsic(post, k);
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            const bool in = (inm >> (2 * k)) & 1u;
+            x[k] = in ? v[k] : x[k];
+            fold(in ? v[k] : 0x00FF00FFu);
+        }
     }
 
     /* combine with the partner thread; the cap at 127 and offset 1, or the
@@ -243,11 +246,12 @@ struct PairCheck {
     __device__ __forceinline__ void write_early(uint16_t* __restrict__ post) const
     {
 #pragma unroll
-        for (int k = 0; k < S; k++)
-            if ((outm >> (2 * k)) & 1u) {
-                uint32_t above, neg;
-                sts16(addr[k], update(k, above, neg));
-            }
+        for (int k = 0; k < S; k++) {
+            uint32_t above, neg;
+            const uint32_t nv = update(k, above, neg);
+            if ((outm >> (2 * k)) & 1u)
+                sts16(addr[k], nv);
+        }
     }
 
     /* every other posterior (predicated stores) and the node's compressed

@@ -72,6 +72,22 @@ bool compile_code(int table, Code* c, std::string* err)
         *err = "group count does not match K";
         return false;
     }
+    /* Within a layer, the entries whose column group occurs more than once
+     * (the only links two checks of the layer can share) go first, in table
+     * order, then the rest.  A check node's result does not depend on the
+     * order of its links (minimums and sign parity are symmetric, each link's
+     * update is its own, and equal minimums give equal messages whichever
+     * link holds the index), so this changes no output; it puts the links the
+     * wavefront levels carry in the first slots. */
+    for (int i = 0; i < q; i++) {
+        auto shared = [&](const std::pair<int, int>& e) {
+            int n = 0;
+            for (auto& f : layer[i])
+                n += f.first == e.first;
+            return n > 1;
+        };
+        std::stable_partition(layer[i].begin(), layer[i].end(), shared);
+    }
 
     c->ent.clear();
     c->eoff.assign(1, 0);

@@ -40,6 +40,9 @@ namespace drxg {
 
 constexpr int kPT = 768; /* threads of a pair CTA */
 constexpr int kQCp = 360;
+/* owned slots 1 .. kLateSlots of each thread (link slots 2 .. 7) can be read
+ * late or written early; codes with shared links beyond run elsewhere */
+constexpr int kLateSlots = 3;
 
 /* PRMT in its default mode: a selector nibble with bit 3 set replicates the
  * sign bit of the selected byte.  (__byte_perm keeps only the low 3 bits of
@@ -101,6 +104,7 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
 template <int DM, bool EXACT>
 struct PairCheck {
     static constexpr int S = (DM + 1) / 2;
+    static constexpr int KL = S - 1 < kLateSlots ? S - 1 : kLateSlots;
     int r;
     uint32_t addr[S]; /* shared-memory byte addresses of the owned links' posteriors */
     uint32_t x[S];
@@ -150,13 +154,12 @@ struct PairCheck {
         sg = 0;
     }
 
-    /* extrinsic input of owned slot k: posterior minus the old message */
-    __device__ __forceinline__ uint32_t extrinsic(const uint16_t* __restrict__ post, int k) const
+    /* minus the old message of owned slot k */
+    __device__ __forceinline__ uint32_t unmsg(int k) const
     {
-        const uint32_t v = sx2(lds16(addr[k]));
         const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(2 * k) * 0x00010001u);
         const uint32_t sm = lmask(sgn << (15 - 2 * k));
-        return sadd(v, sel(sm, sel(im, n1, n0), sel(im, p1, p0)));
+        return sel(sm, sel(im, n1, n0), sel(im, p1, p0));
     }
 
     __device__ __forceinline__ void fold(uint32_t v)
@@ -176,57 +179,89 @@ struct PairCheck {
     __device__ __forceinline__ void read_all(const uint16_t* __restrict__ post)
     {
         const uint32_t excl = LEV ? (~live | inm) : ~live;
+        uint32_t f[S];
 #pragma unroll
         for (int k = 0; k < S; k++) {
-            uint32_t v = extrinsic(post, k);
+            const uint32_t m = unmsg(k);
+            uint32_t v = sadd(sx2(lds16(addr[k])), m);
             if (LEV || !EXACT || k == 0 || (k == S - 1 && (DM & 1)))
                 v = ((excl >> (2 * k)) & 1u) ? 0x00FF00FFu : v;
-            x[k] = v;
+            f[k] = v;
+            /* a late slot keeps minus its old message for read_late */
+            x[k] = LEV && ((inm >> (2 * k)) & 1u) ? m : v;
         }
 #pragma unroll
         for (int k = 0; k + 1 < S; k += 2) {
-            const uint32_t a = abs2(x[k]), b = abs2(x[k + 1]);
+            const uint32_t a = abs2(f[k]), b = abs2(f[k + 1]);
             const uint32_t lo = __vmins2(a, b), hi = __vmaxs2(a, b);
             min1 = __vimin3_s16x2(__vmaxs2(min0, lo), min1, hi);
             min0 = __vimin3_s16x2(min0, a, b);
-            sg ^= x[k] ^ x[k + 1];
+            sg ^= f[k] ^ f[k + 1];
         }
         if (S & 1)
-            fold(x[S - 1]);
+            fold(f[S - 1]);
     }
 
-    /* the late slots (their bits were written by earlier levels) */
-    __device__ __forceinline__ void read_late(const uint16_t* __restrict__ post)
+    /* a thread that holds no check (t >= 720): valid addresses, no links,
+     * so that it can run the warp-uniform level steps of its warp */
+    __device__ __forceinline__ void idle(uint32_t sbase)
     {
-        uint32_t v[S];
-#pragma unroll
-        for (int k = 0; k < S; k++)
-            v[k] = extrinsic(post, k);
+        r = 0;
 #pragma unroll
         for (int k = 0; k < S; k++) {
-            const bool in = (inm >> (2 * k)) & 1u;
-            x[k] = in ? v[k] : x[k];
-            fold(in ? v[k] : 0x00FF00FFu);
+            addr[k] = sbase;
+            x[k] = 0x00FF00FFu;
+        }
+        live = inm = outm = 0;
+        n0 = n1 = p0 = p1 = sgn = 0;
+        idxh = 0x64006400u;
+        min0 = min1 = 0x00FF00FFu;
+        sg = mn0 = mn1 = 0;
+    }
+
+    /* the late slots (their bits were written by earlier levels) of a check
+     * in the current level (mine); other threads keep their state.  Shared
+     * links come first in every layer (codes.cpp), so late and early slots
+     * are among slots 2 .. 2 KL + 1 (owned slots 1 .. KL) */
+    __device__ __forceinline__ void read_late(const uint16_t* __restrict__ post, bool mine)
+    {
+        const uint32_t im = mine ? inm : 0u;
+#pragma unroll
+        for (int k = 1; k <= KL; k++) {
+            const bool in = (im >> (2 * k)) & 1u;
+            const uint32_t v = sadd(sx2(lds16(addr[k])), x[k]);
+            x[k] = in ? v : x[k];
+            fold(in ? v : 0x00FF00FFu);
         }
     }
 
     /* combine with the partner thread; the cap at 127 and offset 1, or the
-     * learned scale and offset of each lane's iteration (lpA, lpB) */
-    __device__ __forceinline__ void finish(unsigned gmask, bool learned, uint32_t lpA, uint32_t lpB)
+     * learned scale and offset of each lane's iteration (lpA, lpB).  Only
+     * threads with `take` keep the result: the level steps run it on whole
+     * warps (full-mask shuffles; a shuffle under a partial mask inside a
+     * divergent branch costs several times as much) */
+    __device__ __forceinline__ void finish(unsigned gmask, bool take, bool learned, uint32_t lpA, uint32_t lpB)
     {
         const uint32_t b0 = __shfl_xor_sync(gmask, min0, 1);
         const uint32_t b1 = __shfl_xor_sync(gmask, min1, 1);
         const uint32_t bs = __shfl_xor_sync(gmask, sg, 1);
-        min1 = __vmins2(__vmaxs2(min0, b0), __vmins2(min1, b1));
-        min0 = __vmins2(min0, b0);
-        sg ^= bs;
+        const uint32_t c1 = __vmins2(__vmaxs2(min0, b0), __vmins2(min1, b1));
+        const uint32_t c0 = __vmins2(min0, b0);
+        uint32_t m0, m1;
         if (learned) {
-            const uint32_t c0 = __vmins2(min0, 0x007F007Fu), c1 = __vmins2(min1, 0x007F007Fu);
-            mn0 = (uint32_t)learned_mag(c0 & 0xFFFF, lpA) | (uint32_t)learned_mag(c0 >> 16, lpB) << 16;
-            mn1 = (uint32_t)learned_mag(c1 & 0xFFFF, lpA) | (uint32_t)learned_mag(c1 >> 16, lpB) << 16;
+            const uint32_t k0 = __vmins2(c0, 0x007F007Fu), k1 = __vmins2(c1, 0x007F007Fu);
+            m0 = (uint32_t)learned_mag(k0 & 0xFFFF, lpA) | (uint32_t)learned_mag(k0 >> 16, lpB) << 16;
+            m1 = (uint32_t)learned_mag(k1 & 0xFFFF, lpA) | (uint32_t)learned_mag(k1 >> 16, lpB) << 16;
         } else {
-            mn0 = __viaddmax_s16x2(__vmins2(min0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
-            mn1 = __viaddmax_s16x2(__vmins2(min1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+            m0 = __viaddmax_s16x2(__vmins2(c0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+            m1 = __viaddmax_s16x2(__vmins2(c1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+        }
+        if (take) {
+            min0 = c0;
+            min1 = c1;
+            sg ^= bs;
+            mn0 = m0;
+            mn1 = m1;
         }
     }
 
@@ -242,14 +277,16 @@ struct PairCheck {
         return pk2(sadd(v, o));
     }
 
-    /* posteriors that later levels of the layer read */
-    __device__ __forceinline__ void write_early(uint16_t* __restrict__ post) const
+    /* posteriors that later levels of the layer read (checks of the current
+     * level only) */
+    __device__ __forceinline__ void write_early(uint16_t* __restrict__ post, bool mine) const
     {
+        const uint32_t om = mine ? outm : 0u;
 #pragma unroll
-        for (int k = 0; k < S; k++) {
+        for (int k = 1; k <= KL; k++) {
             uint32_t above, neg;
             const uint32_t nv = update(k, above, neg);
-            if ((outm >> (2 * k)) & 1u)
+            if ((om >> (2 * k)) & 1u)
                 sts16(addr[k], nv);
         }
     }
@@ -431,19 +468,22 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             ck.template read_all<true>(fr.post);
         else
             ck.template read_all<false>(fr.post);
+    } else {
+        ck.idle((uint32_t)__cvta_generic_to_shared(fr.post));
     }
     if (nlev > 1) {
-        const int lev = (int)(meta & 0xFF);
+        /* a level step runs on every warp that holds a check of the level,
+         * with all its lanes; the other checks keep their state */
+        const int lev = active ? (int)(meta & 0xFF) : -1;
         for (int l = 0; l < nlev; l++) {
-            const bool mine = active && lev == l;
-            const unsigned gm = __ballot_sync(0xFFFFFFFFu, mine);
-            if (mine) {
+            const bool mine = lev == l;
+            if (__any_sync(0xFFFFFFFFu, mine)) {
                 if (l > 0)
-                    ck.read_late(fr.post);
+                    ck.read_late(fr.post, mine);
                 uint32_t wa, wb;
                 lwords(wa, wb);
-                ck.finish(gm, lA >= 0, wa, wb);
-                ck.write_early(fr.post);
+                ck.finish(0xFFFFFFFFu, mine, lA >= 0, wa, wb);
+                ck.write_early(fr.post, mine);
             }
             __syncthreads();
         }
@@ -452,7 +492,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
         if (active) {
             uint32_t wa, wb;
             lwords(wa, wb);
-            ck.finish(gm, lA >= 0, wa, wb);
+            ck.finish(gm, true, lA >= 0, wa, wb);
         }
     }
     const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
@@ -624,6 +664,10 @@ int pair_kernel_id(const Code& c)
 {
     if (c.deg_max > 14)
         return -1;
+    /* late / early slots only among link slots 2 .. 2 kLateSlots + 1 */
+    for (uint64_t m : c.lmeta)
+        if ((((m >> 8) | (m >> 32)) & 0xFFFFFFull) >> (2 * kLateSlots + 2))
+            return -1;
     int lo = 1 << 30, hi = 0, other = 0;
     for (int i = 0; i < c.q; i++) {
         const int n = c.eoff[i + 1] - c.eoff[i];

@@ -443,7 +443,7 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
  * constrain the bits two checks of a layer share, so the wavefront levels
  * carry just those links.  Unlevelled layers take one pass.
  */
-template <int DM, bool EXACT>
+template <int DM, bool EXACT, bool LEARNED>
 __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev, uint2 rec,
                                            unsigned long long meta, uint32_t fresh, uint2* __restrict__ msg,
                                            int lA, int lB)
@@ -454,7 +454,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
     /* learned scale / offset words of the check for both lanes */
     auto lwords = [&](uint32_t& a, uint32_t& b) {
         a = b = 0;
-        if (lA >= 0) {
+        if (LEARNED) {
             const int k = s_learn_cls[(EXACT ? DM : cnt + 2) - ((i | j) == 0)];
             a = s_learn_tab[lA + k];
             b = s_learn_tab[lB + k];
@@ -482,7 +482,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
                     ck.read_late(fr.post, mine);
                 uint32_t wa, wb;
                 lwords(wa, wb);
-                ck.finish(0xFFFFFFFFu, mine, lA >= 0, wa, wb);
+                ck.finish(0xFFFFFFFFu, mine, LEARNED, wa, wb);
                 ck.write_early(fr.post, mine);
             }
             __syncthreads();
@@ -492,7 +492,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
         if (active) {
             uint32_t wa, wb;
             lwords(wa, wb);
-            ck.finish(gm, true, lA >= 0, wa, wb);
+            ck.finish(gm, true, LEARNED, wa, wb);
         }
     }
     const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
@@ -505,7 +505,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
  * level metadata are fetched one layer ahead.  The kernel is compiled for
  * the two information-link counts A <= B of its codes (exact-degree check
  * nodes), or, with GDM > 0, for any count up to GDM - 2 (predicated). */
-template <int A, int B, int GDM>
+template <int A, int B, int GDM, bool LEARNED>
 __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __restrict__ msg, uint32_t fresh,
                              int lA, int lB)
 {
@@ -528,11 +528,11 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __res
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
         const int nlev = c.nlev[i];
         if (GDM > 0)
-            layer_pair<(GDM > 0 ? GDM : 2), false>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<(GDM > 0 ? GDM : 2), false, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else if (A == B || cnt == A)
-            layer_pair<A + 2, true>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<A + 2, true, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else
-            layer_pair<B + 2, true>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<B + 2, true, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
     }
 }
 
@@ -620,8 +620,10 @@ __global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
         __syncthreads();
         if (done)
             continue; /* reload, then check the new frames first */
-        iterate_pair<A, B, GDM>(c, fr, msg, fresh, lT ? learn_row(s_iter[0], lT) : -1,
-                                lT ? learn_row(s_iter[1], lT) : -1);
+        if (lT)
+            iterate_pair<A, B, GDM, true>(c, fr, msg, fresh, learn_row(s_iter[0], lT), learn_row(s_iter[1], lT));
+        else
+            iterate_pair<A, B, GDM, false>(c, fr, msg, fresh, -1, -1);
         fresh = 0;
         if (t == 0) {
             s_iter[0]++;

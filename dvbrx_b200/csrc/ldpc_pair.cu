@@ -40,9 +40,10 @@ namespace drxg {
 
 constexpr int kPT = 768; /* threads of a pair CTA */
 constexpr int kQCp = 360;
-/* owned slots 1 .. kLateSlots of each thread (link slots 2 .. 7) can be read
- * late or written early; codes with shared links beyond run elsewhere */
-constexpr int kLateSlots = 3;
+/* a kernel compiled for LS late slots reads late and writes early only owned
+ * slots 1 .. LS of each thread (link slots 2 .. 2 LS + 1); two cover every
+ * pair code but short 3/5 and 4/5, which take three */
+constexpr int kLateSlotsMax = 3;
 
 /* PRMT in its default mode: a selector nibble with bit 3 set replicates the
  * sign bit of the selected byte.  (__byte_perm keeps only the low 3 bits of
@@ -101,10 +102,10 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
  * in its level), enters the minimums as 255, which no magnitude reaches;
  * stores are predicated.
  */
-template <int DM, bool EXACT>
+template <int DM, bool EXACT, int LS>
 struct PairCheck {
     static constexpr int S = (DM + 1) / 2;
-    static constexpr int KL = S - 1 < kLateSlots ? S - 1 : kLateSlots;
+    static constexpr int KL = S - 1 < LS ? S - 1 : LS;
     int r;
     uint32_t addr[S]; /* shared-memory byte addresses of the owned links' posteriors */
     uint32_t x[S];
@@ -443,7 +444,7 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
  * constrain the bits two checks of a layer share, so the wavefront levels
  * carry just those links.  Unlevelled layers take one pass.
  */
-template <int DM, bool EXACT, bool LEARNED>
+template <int DM, bool EXACT, int LS, bool LEARNED>
 __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev, uint2 rec,
                                            unsigned long long meta, uint32_t fresh, uint2* __restrict__ msg,
                                            int lA, int lB)
@@ -460,7 +461,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             b = s_learn_tab[lB + k];
         }
     };
-    PairCheck<DM, EXACT> ck;
+    PairCheck<DM, EXACT, LS> ck;
     if (active) {
         ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, t & 1, rec, fresh, meta,
                  (uint32_t)__cvta_generic_to_shared(fr.post));
@@ -505,7 +506,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
  * level metadata are fetched one layer ahead.  The kernel is compiled for
  * the two information-link counts A <= B of its codes (exact-degree check
  * nodes), or, with GDM > 0, for any count up to GDM - 2 (predicated). */
-template <int A, int B, int GDM, bool LEARNED>
+template <int A, int B, int GDM, int LS, bool LEARNED>
 __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __restrict__ msg, uint32_t fresh,
                              int lA, int lB)
 {
@@ -528,11 +529,11 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __res
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
         const int nlev = c.nlev[i];
         if (GDM > 0)
-            layer_pair<(GDM > 0 ? GDM : 2), false, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<(GDM > 0 ? GDM : 2), false, LS, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else if (A == B || cnt == A)
-            layer_pair<A + 2, true, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<A + 2, true, LS, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else
-            layer_pair<B + 2, true, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<B + 2, true, LS, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
     }
 }
 
@@ -551,7 +552,7 @@ __device__ void store_lane(const DevCode& c, const PairFrame& fr, int h, uint8_t
     }
 }
 
-template <int A, int B, int GDM>
+template <int A, int B, int GDM, int LS>
 __global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
 {
     extern __shared__ __align__(16) char smem[];
@@ -621,9 +622,9 @@ __global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
         if (done)
             continue; /* reload, then check the new frames first */
         if (lT)
-            iterate_pair<A, B, GDM, true>(c, fr, msg, fresh, learn_row(s_iter[0], lT), learn_row(s_iter[1], lT));
+            iterate_pair<A, B, GDM, LS, true>(c, fr, msg, fresh, learn_row(s_iter[0], lT), learn_row(s_iter[1], lT));
         else
-            iterate_pair<A, B, GDM, false>(c, fr, msg, fresh, -1, -1);
+            iterate_pair<A, B, GDM, LS, false>(c, fr, msg, fresh, -1, -1);
         fresh = 0;
         if (t == 0) {
             s_iter[0]++;
@@ -646,19 +647,21 @@ size_t decode_pair_msg_bytes(int R) { return (size_t)R * sizeof(uint2); }
  * S2X and T2 codes up to check degree 14, plus predicated kernels for the
  * codes whose layers have more than two different counts. */
 struct PairKernel {
-    int a, b, gdm;
+    int a, b, gdm, ls;
     const void* fn;
 };
 
-#define DRXG_PK(a, b) { a, b, 0, (const void*)k_decode_pair<a, b, 0> }
-#define DRXG_PG(d) { 0, 0, d, (const void*)k_decode_pair<1, 1, d> }
+#define DRXG_PK(a, b) { a, b, 0, 2, (const void*)k_decode_pair<a, b, 0, 2> }
+#define DRXG_PK3(a, b) { a, b, 0, 3, (const void*)k_decode_pair<a, b, 0, 3> }
+#define DRXG_PG(d) { 0, 0, d, 3, (const void*)k_decode_pair<1, 1, d, 3> }
 static const PairKernel kPairKernels[] = {
     DRXG_PK(1, 2), DRXG_PK(2, 2), DRXG_PK(2, 3), DRXG_PK(3, 3), DRXG_PK(4, 4), DRXG_PK(5, 5),
     DRXG_PK(5, 6), DRXG_PK(6, 7), DRXG_PK(7, 7), DRXG_PK(7, 8), DRXG_PK(8, 8), DRXG_PK(8, 9),
-    DRXG_PK(9, 9), DRXG_PK(9, 10), DRXG_PK(11, 11), DRXG_PK(11, 12), DRXG_PK(12, 12),
+    DRXG_PK(9, 9), DRXG_PK(9, 10), DRXG_PK(11, 11), DRXG_PK(11, 12), DRXG_PK(12, 12), DRXG_PK3(9, 9),
     DRXG_PG(7), DRXG_PG(11), DRXG_PG(14),
 };
 #undef DRXG_PK
+#undef DRXG_PK3
 #undef DRXG_PG
 constexpr int kNumPairKernels = (int)(sizeof(kPairKernels) / sizeof(kPairKernels[0]));
 
@@ -666,10 +669,15 @@ int pair_kernel_id(const Code& c)
 {
     if (c.deg_max > 14)
         return -1;
-    /* late / early slots only among link slots 2 .. 2 kLateSlots + 1 */
-    for (uint64_t m : c.lmeta)
-        if ((((m >> 8) | (m >> 32)) & 0xFFFFFFull) >> (2 * kLateSlots + 2))
-            return -1;
+    /* late slots the code needs: link slots 2 .. 2 ls + 1 */
+    int ls = 0;
+    for (uint64_t m : c.lmeta) {
+        const uint32_t b = (uint32_t)(((m >> 8) | (m >> 32)) & 0xFFFFFFull);
+        while (b >> (2 * ls + 2))
+            ls++;
+    }
+    if (ls > kLateSlotsMax)
+        return -1;
     int lo = 1 << 30, hi = 0, other = 0;
     for (int i = 0; i < c.q; i++) {
         const int n = c.eoff[i + 1] - c.eoff[i];
@@ -682,10 +690,11 @@ int pair_kernel_id(const Code& c)
     }
     if (!other)
         for (int k = 0; k < kNumPairKernels; k++)
-            if (kPairKernels[k].gdm == 0 && kPairKernels[k].a == lo && kPairKernels[k].b == hi)
+            if (kPairKernels[k].gdm == 0 && kPairKernels[k].a == lo && kPairKernels[k].b == hi &&
+                kPairKernels[k].ls >= ls)
                 return k;
     for (int k = 0; k < kNumPairKernels; k++)
-        if (kPairKernels[k].gdm >= c.deg_max)
+        if (kPairKernels[k].gdm >= c.deg_max && kPairKernels[k].ls >= ls)
             return k;
     return -1;
 }

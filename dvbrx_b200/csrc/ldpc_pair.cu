@@ -14,14 +14,16 @@
  * v holds the int8 posterior of variable v for lane A (low byte) and lane B
  * (high byte): K information bits, then R parity bits in layer order.
  *
- * A check node runs on two threads (its links alternate between them), which
- * combine their two smallest magnitudes and sign parities with one shuffle
- * round; 720 of the 768 threads hold the 360 checks of a layer.  Levelled
- * layers run in phases (layer_pair): the wavefront levels carry only the
- * links two checks of the layer share.  The first thread of a check stores
- * its compressed messages for both frames in one 8-byte record: per lane
- * min0 (6 bits) | min1 << 6 | index << 12, then the sign bits of lane A in
- * the low half and of lane B in the high half.
+ * A check node runs on one thread (T = 1): 360 of the 384 threads hold the
+ * 360 checks of a layer, every link of a check in registers, no shuffles.
+ * (The template also builds T = 2, a check's links alternating over two
+ * threads that combine their minimums with one shuffle round; on 3/5 and
+ * 18/30 it runs 17-22 % slower: twice the per-check set-up and finish work
+ * for the same link work.)  Levelled layers run in phases (layer_pair): the
+ * wavefront levels carry only the links two checks of the layer share.  The
+ * thread of a check stores its compressed messages for both frames in one
+ * 8-byte record: per lane min0 (6 bits) | min1 << 6 | index << 12, then the
+ * sign bits of lane A in the low half and of lane B in the high half.
  *
  * Frames stream through the two lanes independently: when a lane's frame
  * passes the syndrome check or reaches max_iter, its results are written
@@ -38,7 +40,6 @@
 
 namespace drxg {
 
-constexpr int kPT = 768; /* threads of a pair CTA */
 constexpr int kQCp = 360;
 /* a kernel compiled for LS late slots reads late and writes early only owned
  * slots 1 .. LS of each thread (link slots 2 .. 2 LS + 1); two cover every
@@ -87,14 +88,14 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
 }
 
 /*
- * One check node (i, j) for both lanes, on two threads (r = 0, 1): thread r
- * owns the node's link slots c = r + 2k, k = 0 .. S-1.  Slot 0 is the
+ * One check node (i, j) for both lanes, on T threads (r = 0 .. T-1): thread
+ * r owns the node's link slots c = r + T k, k = 0 .. S-1.  Slot 0 is the
  * parity bit, slot 1 the previous parity bit (absent for (0, 0)), 2 + e
  * information entry e of the layer.  DM is the node degree (EXACT) or a
  * bound on it (the degree is then a run-time value).  The node state lives
  * in registers across the phases of its layer (see layer_pair).
  *
- * Slot masks keep owned slot k at bit 2k (the layer's 24-bit slot masks
+ * Slot masks keep owned slot k at bit T k (the layer's 24-bit slot masks
  * shifted right by r); the message's sign bits and index are shifted by r
  * the same way, so everything a slot needs besides its address depends on
  * k alone.  The full passes run every slot without branches: a slot that is
@@ -102,10 +103,12 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
  * in its level), enters the minimums as 255, which no magnitude reaches;
  * stores are predicated.
  */
-template <int DM, bool EXACT, int LS>
+template <int DM, bool EXACT, int LS, int T>
 struct PairCheck {
-    static constexpr int S = (DM + 1) / 2;
-    static constexpr int KL = S - 1 < LS ? S - 1 : LS;
+    static constexpr int S = T == 2 ? (DM + 1) / 2 : DM;
+    /* owned slots that can be late or early: k0 .. k1 (link slots 2 .. 2 LS + 1) */
+    static constexpr int K0 = T == 2 ? 1 : 2;
+    static constexpr int K1 = T == 2 ? (S - 1 < LS ? S - 1 : LS) : (S - 1 < 2 * LS + 1 ? S - 1 : 2 * LS + 1);
     int r;
     uint32_t addr[S]; /* shared-memory byte addresses of the owned links' posteriors */
     uint32_t x[S];
@@ -129,17 +132,16 @@ struct PairCheck {
         outm = ((uint32_t)(meta >> 32) & 0xFFFFFFu) >> r;
 #pragma unroll
         for (int k = 0; k < S; k++) {
-            const int c = r + 2 * k;
-            int a;
-            if (k == 0) {
-                a = r == 0 ? pc : pp;
+            const int c = r + T * k;
+            if (T == 2 && k == 0) {
+                addr[k] = sbase + 2u * (uint32_t)(r == 0 ? pc : pp);
+            } else if (T == 1 && k < 2) {
+                addr[k] = sbase + 2u * (uint32_t)(k == 0 ? pc : pp);
             } else {
                 /* a slot past the degree takes the last link's address: read, never used */
                 const int2 e = ent[min(c, D - 1) - 2];
                 addr[k] = (uint32_t)e.x + 2u * (uint32_t)j + (j < e.y ? 2u * kQCp : 0u);
-                continue;
             }
-            addr[k] = sbase + 2u * (uint32_t)a;
         }
         /* messages: zero for a lane in its first iteration */
         const uint32_t w0 = rec.x & ~fresh;
@@ -158,8 +160,8 @@ struct PairCheck {
     /* minus the old message of owned slot k */
     __device__ __forceinline__ uint32_t unmsg(int k) const
     {
-        const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(2 * k) * 0x00010001u);
-        const uint32_t sm = lmask(sgn << (15 - 2 * k));
+        const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(T * k) * 0x00010001u);
+        const uint32_t sm = lmask(sgn << (15 - T * k));
         return sel(sm, sel(im, n1, n0), sel(im, p1, p0));
     }
 
@@ -185,11 +187,11 @@ struct PairCheck {
         for (int k = 0; k < S; k++) {
             const uint32_t m = unmsg(k);
             uint32_t v = sadd(sx2(lds16(addr[k])), m);
-            if (LEV || !EXACT || k == 0 || (k == S - 1 && (DM & 1)))
-                v = ((excl >> (2 * k)) & 1u) ? 0x00FF00FFu : v;
+            if (LEV || !EXACT || (T == 2 ? k == 0 || (k == S - 1 && (DM & 1)) : k == 1))
+                v = ((excl >> (T * k)) & 1u) ? 0x00FF00FFu : v;
             f[k] = v;
             /* a late slot keeps minus its old message for read_late */
-            x[k] = LEV && ((inm >> (2 * k)) & 1u) ? m : v;
+            x[k] = LEV && ((inm >> (T * k)) & 1u) ? m : v;
         }
 #pragma unroll
         for (int k = 0; k + 1 < S; k += 2) {
@@ -203,7 +205,7 @@ struct PairCheck {
             fold(f[S - 1]);
     }
 
-    /* a thread that holds no check (t >= 720): valid addresses, no links,
+    /* a thread that holds no check (t >= 360 T): valid addresses, no links,
      * so that it can run the warp-uniform level steps of its warp */
     __device__ __forceinline__ void idle(uint32_t sbase)
     {
@@ -228,24 +230,24 @@ struct PairCheck {
     {
         const uint32_t im = mine ? inm : 0u;
 #pragma unroll
-        for (int k = 1; k <= KL; k++) {
-            const bool in = (im >> (2 * k)) & 1u;
+        for (int k = K0; k <= K1; k++) {
+            const bool in = (im >> (T * k)) & 1u;
             const uint32_t v = sadd(sx2(lds16(addr[k])), x[k]);
             x[k] = in ? v : x[k];
             fold(in ? v : 0x00FF00FFu);
         }
     }
 
-    /* combine with the partner thread; the cap at 127 and offset 1, or the
+    /* combine with the partner thread (T = 2); the cap at 127 and offset 1, or the
      * learned scale and offset of each lane's iteration (lpA, lpB).  Only
      * threads with `take` keep the result: the level steps run it on whole
      * warps (full-mask shuffles; a shuffle under a partial mask inside a
      * divergent branch costs several times as much) */
     __device__ __forceinline__ void finish(unsigned gmask, bool take, bool learned, uint32_t lpA, uint32_t lpB)
     {
-        const uint32_t b0 = __shfl_xor_sync(gmask, min0, 1);
-        const uint32_t b1 = __shfl_xor_sync(gmask, min1, 1);
-        const uint32_t bs = __shfl_xor_sync(gmask, sg, 1);
+        const uint32_t b0 = T == 2 ? __shfl_xor_sync(gmask, min0, 1) : 0x00FF00FFu;
+        const uint32_t b1 = T == 2 ? __shfl_xor_sync(gmask, min1, 1) : 0x00FF00FFu;
+        const uint32_t bs = T == 2 ? __shfl_xor_sync(gmask, sg, 1) : 0u;
         const uint32_t c1 = __vmins2(__vmaxs2(min0, b0), __vmins2(min1, b1));
         const uint32_t c0 = __vmins2(min0, b0);
         uint32_t m0, m1;
@@ -284,10 +286,10 @@ struct PairCheck {
     {
         const uint32_t om = mine ? outm : 0u;
 #pragma unroll
-        for (int k = 1; k <= KL; k++) {
+        for (int k = K0; k <= K1; k++) {
             uint32_t above, neg;
             const uint32_t nv = update(k, above, neg);
-            if ((om >> (2 * k)) & 1u)
+            if ((om >> (T * k)) & 1u)
                 sts16(addr[k], nv);
         }
     }
@@ -298,22 +300,24 @@ struct PairCheck {
     __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, unsigned gmask, uint2* __restrict__ dst)
     {
         const uint32_t wm = live & ~outm;
-        uint32_t nidx = 0, nsg = 0; /* nidx per lane: 2k + 1 of an owned slot holding min0, 0 if none */
+        uint32_t nidx = 0, nsg = 0; /* nidx per lane: T k + 1 of an owned slot holding min0, 0 if none */
 #pragma unroll
         for (int k = 0; k < S; k++) {
             uint32_t above, neg;
             const uint32_t nv = update(k, above, neg);
-            if ((wm >> (2 * k)) & 1u)
+            if ((wm >> (T * k)) & 1u)
                 sts16(addr[k], nv);
-            nidx = sel(above, nidx, (uint32_t)(2 * k + 1) * 0x00010001u);
-            nsg |= neg & (0x00010001u << (2 * k));
+            nidx = sel(above, nidx, (uint32_t)(T * k + 1) * 0x00010001u);
+            nsg |= neg & (0x00010001u << (T * k));
         }
-        nsg <<= r; /* bit 2k -> slot 2k + r (slots stay below 16: no carry across lanes) */
-        const uint32_t found = lmask(__vsub2(0u, nidx)); /* lanes with nidx > 0 */
-        nidx = __vadd2(nidx, found & ((uint32_t)r * 0x00010001u)); /* 2k + r + 1 */
-        nidx = __vmaxs2(nidx, __shfl_xor_sync(gmask, nidx, 1));
+        if (T == 2) {
+            nsg <<= r; /* bit 2k -> slot 2k + r (slots stay below 16: no carry across lanes) */
+            const uint32_t found = lmask(__vsub2(0u, nidx)); /* lanes with nidx > 0 */
+            nidx = __vadd2(nidx, found & ((uint32_t)r * 0x00010001u)); /* 2k + r + 1 */
+            nidx = __vmaxs2(nidx, __shfl_xor_sync(gmask, nidx, 1));
+            nsg |= __shfl_xor_sync(gmask, nsg, 1);
+        }
         nidx = __vmaxs2(__vsub2(nidx, 0x00010001u), 0u); /* slot number */
-        nsg |= __shfl_xor_sync(gmask, nsg, 1);
         if (r == 0) {
             const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
             __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
@@ -444,14 +448,14 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
  * constrain the bits two checks of a layer share, so the wavefront levels
  * carry just those links.  Unlevelled layers take one pass.
  */
-template <int DM, bool EXACT, int LS, bool LEARNED>
+template <int DM, bool EXACT, int LS, int T, bool LEARNED>
 __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev, uint2 rec,
                                            unsigned long long meta, uint32_t fresh, uint2* __restrict__ msg,
                                            int lA, int lB)
 {
     const int t = threadIdx.x;
-    const bool active = t < 2 * kQCp;
-    const int j = t >> 1;
+    const bool active = t < T * kQCp;
+    const int j = T == 2 ? t >> 1 : t;
     /* learned scale / offset words of the check for both lanes */
     auto lwords = [&](uint32_t& a, uint32_t& b) {
         a = b = 0;
@@ -461,9 +465,9 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             b = s_learn_tab[lB + k];
         }
     };
-    PairCheck<DM, EXACT, LS> ck;
+    PairCheck<DM, EXACT, LS, T> ck;
     if (active) {
-        ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, t & 1, rec, fresh, meta,
+        ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, T == 2 ? t & 1 : 0, rec, fresh, meta,
                  (uint32_t)__cvta_generic_to_shared(fr.post));
         if (nlev > 1)
             ck.template read_all<true>(fr.post);
@@ -506,13 +510,13 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
  * level metadata are fetched one layer ahead.  The kernel is compiled for
  * the two information-link counts A <= B of its codes (exact-degree check
  * nodes), or, with GDM > 0, for any count up to GDM - 2 (predicated). */
-template <int A, int B, int GDM, int LS, bool LEARNED>
+template <int A, int B, int GDM, int LS, int T, bool LEARNED>
 __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __restrict__ msg, uint32_t fresh,
                              int lA, int lB)
 {
     const int t = threadIdx.x;
-    const int j = t >> 1;
-    const bool active = t < 2 * kQCp;
+    const int j = T == 2 ? t >> 1 : t;
+    const bool active = t < T * kQCp;
     uint2 rn = make_uint2(0, 0);
     unsigned long long mn = 0;
     if (active) {
@@ -529,11 +533,11 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __res
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
         const int nlev = c.nlev[i];
         if (GDM > 0)
-            layer_pair<(GDM > 0 ? GDM : 2), false, LS, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<(GDM > 0 ? GDM : 2), false, LS, T, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else if (A == B || cnt == A)
-            layer_pair<A + 2, true, LS, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<A + 2, true, LS, T, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else
-            layer_pair<B + 2, true, LS, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<B + 2, true, LS, T, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
     }
 }
 
@@ -552,8 +556,8 @@ __device__ void store_lane(const DevCode& c, const PairFrame& fr, int h, uint8_t
     }
 }
 
-template <int A, int B, int GDM, int LS>
-__global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
+template <int A, int B, int GDM, int LS, int T>
+__global__ void __launch_bounds__(T * 384, 1) k_decode_pair(DecodeParams p)
 {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_frame[2], s_iter[2], s_flag, s_reload;
@@ -622,9 +626,9 @@ __global__ void __launch_bounds__(kPT, 1) k_decode_pair(DecodeParams p)
         if (done)
             continue; /* reload, then check the new frames first */
         if (lT)
-            iterate_pair<A, B, GDM, LS, true>(c, fr, msg, fresh, learn_row(s_iter[0], lT), learn_row(s_iter[1], lT));
+            iterate_pair<A, B, GDM, LS, T, true>(c, fr, msg, fresh, learn_row(s_iter[0], lT), learn_row(s_iter[1], lT));
         else
-            iterate_pair<A, B, GDM, LS, false>(c, fr, msg, fresh, -1, -1);
+            iterate_pair<A, B, GDM, LS, T, false>(c, fr, msg, fresh, -1, -1);
         fresh = 0;
         if (t == 0) {
             s_iter[0]++;
@@ -647,13 +651,13 @@ size_t decode_pair_msg_bytes(int R) { return (size_t)R * sizeof(uint2); }
  * S2X and T2 codes up to check degree 14, plus predicated kernels for the
  * codes whose layers have more than two different counts. */
 struct PairKernel {
-    int a, b, gdm, ls;
+    int a, b, gdm, ls, threads;
     const void* fn;
 };
 
-#define DRXG_PK(a, b) { a, b, 0, 2, (const void*)k_decode_pair<a, b, 0, 2> }
-#define DRXG_PK3(a, b) { a, b, 0, 3, (const void*)k_decode_pair<a, b, 0, 3> }
-#define DRXG_PG(d) { 0, 0, d, 3, (const void*)k_decode_pair<1, 1, d, 3> }
+#define DRXG_PK(a, b) { a, b, 0, 2, 384, (const void*)k_decode_pair<a, b, 0, 2, 1> }
+#define DRXG_PK3(a, b) { a, b, 0, 3, 384, (const void*)k_decode_pair<a, b, 0, 3, 1> }
+#define DRXG_PG(d) { 0, 0, d, 3, 384, (const void*)k_decode_pair<1, 1, d, 3, 1> }
 static const PairKernel kPairKernels[] = {
     DRXG_PK(1, 2), DRXG_PK(2, 2), DRXG_PK(2, 3), DRXG_PK(3, 3), DRXG_PK(4, 4), DRXG_PK(5, 5),
     DRXG_PK(5, 6), DRXG_PK(6, 7), DRXG_PK(7, 7), DRXG_PK(7, 8), DRXG_PK(8, 8), DRXG_PK(8, 9),
@@ -707,7 +711,7 @@ int decode_pair_ctas_per_sm(int kid, size_t smem)
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kPT, smem) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kPairKernels[kid].threads, smem) != cudaSuccess)
         return 0;
     return n;
 }
@@ -722,7 +726,7 @@ cudaError_t launch_decode_pair(const DecodeParams& p, int kid, size_t smem, int 
         return e;
     DecodeParams pc = p;
     void* args[] = { &pc };
-    return cudaLaunchKernel(k, dim3(grid), dim3(kPT), args, smem, stream);
+    return cudaLaunchKernel(k, dim3(grid), dim3(kPairKernels[kid].threads), args, smem, stream);
 }
 
 }  // namespace drxg

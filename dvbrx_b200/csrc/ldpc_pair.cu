@@ -35,6 +35,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "codes.h"
 #include "ldpc_device.h"
 
@@ -226,11 +228,12 @@ struct PairCheck {
      * in the current level (mine); other threads keep their state.  Shared
      * links come first in every layer (codes.cpp), so late and early slots
      * are among slots 2 .. 2 KL + 1 (owned slots 1 .. KL) */
+    template <int KE>
     __device__ __forceinline__ void read_late(const uint16_t* __restrict__ post, bool mine)
     {
         const uint32_t im = mine ? inm : 0u;
 #pragma unroll
-        for (int k = K0; k <= K1; k++) {
+        for (int k = K0; k <= KE; k++) {
             const bool in = (im >> (T * k)) & 1u;
             const uint32_t v = sadd(sx2(lds16(addr[k])), x[k]);
             x[k] = in ? v : x[k];
@@ -282,11 +285,12 @@ struct PairCheck {
 
     /* posteriors that later levels of the layer read (checks of the current
      * level only) */
+    template <int KE>
     __device__ __forceinline__ void write_early(uint16_t* __restrict__ post, bool mine) const
     {
         const uint32_t om = mine ? outm : 0u;
 #pragma unroll
-        for (int k = K0; k <= K1; k++) {
+        for (int k = K0; k <= KE; k++) {
             uint32_t above, neg;
             const uint32_t nv = update(k, above, neg);
             if ((om >> (T * k)) & 1u)
@@ -478,20 +482,32 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
     }
     if (nlev > 1) {
         /* a level step runs on every warp that holds a check of the level,
-         * with all its lanes; the other checks keep their state */
+         * with all its lanes; the other checks keep their state.  KE: the
+         * last owned slot that can be late or early in this warp (most
+         * layers share one pair of links: link slots 2 and 3 only) */
         const int lev = active ? (int)(meta & 0xFF) : -1;
-        for (int l = 0; l < nlev; l++) {
-            const bool mine = lev == l;
-            if (__any_sync(0xFFFFFFFFu, mine)) {
-                if (l > 0)
-                    ck.read_late(fr.post, mine);
-                uint32_t wa, wb;
-                lwords(wa, wb);
-                ck.finish(0xFFFFFFFFu, mine, LEARNED, wa, wb);
-                ck.write_early(fr.post, mine);
+        auto steps = [&](auto ke) {
+            constexpr int KE = decltype(ke)::value;
+            for (int l = 0; l < nlev; l++) {
+                const bool mine = lev == l;
+                if (__any_sync(0xFFFFFFFFu, mine)) {
+                    if (l > 0)
+                        ck.template read_late<KE>(fr.post, mine);
+                    uint32_t wa, wb;
+                    lwords(wa, wb);
+                    ck.finish(0xFFFFFFFFu, mine, LEARNED, wa, wb);
+                    ck.template write_early<KE>(fr.post, mine);
+                }
+                __syncthreads();
             }
-            __syncthreads();
-        }
+        };
+        using Ck = PairCheck<DM, EXACT, LS, T>;
+        constexpr int KS = T == 1 && Ck::K1 > 3 ? 3 : Ck::K1;
+        const uint32_t lm = __reduce_or_sync(0xFFFFFFFFu, ck.inm | ck.outm);
+        if (KS < Ck::K1 && (lm >> (T * (KS + 1))) != 0)
+            steps(std::integral_constant<int, Ck::K1>());
+        else
+            steps(std::integral_constant<int, KS>());
     } else {
         const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
         if (active) {

@@ -6,7 +6,7 @@
  * 32-bit register carries the same quantity for two frames, lane A in the
  * low half and lane B in the high half, and every step of the check node is
  * a native 16x2 instruction on sm_100a (video min/max __vmins2/__vmaxs2,
- * DPX __viaddmax_s16x2 for the saturating add, lane-wise __vsub2/__vneg2,
+ * DPX __viaddmax_s16x2 for the saturating add and |x|, the lane-wise __vadd2,
  * PRMT for sign masks and byte packing, an FP16 compare for the message
  * index).  One instruction stream decodes two frames.
  *
@@ -69,10 +69,11 @@ __device__ __forceinline__ uint32_t sadd(uint32_t a, uint32_t b)
 {
     return __vmins2(__viaddmax_s16x2(a, b, 0xFF80FF80u), 0x007F007Fu);
 }
-/* lane-wise negation and |x|: __vsub2 issues on the FMA pipe, leaving the
- * (half-rate) ALU pipe to the min/max, select and permute work */
-__device__ __forceinline__ uint32_t neg2(uint32_t x) { return __vsub2(0u, x); }
-__device__ __forceinline__ uint32_t abs2(uint32_t x) { return __vmaxs2(x, neg2(x)); }
+/* lane-wise |x| = max(~x + 1, x): one LOP3 and one DPX add-max (a 16x2
+ * subtract, __vsub2, has no single instruction: it costs three or four) */
+__device__ __forceinline__ uint32_t abs2(uint32_t x) { return __viaddmax_s16x2(~x, 0x00010001u, x); }
+/* lane-wise -x, the 16x2 add (__vadd2) being one instruction */
+__device__ __forceinline__ uint32_t neg2(uint32_t x) { return __vadd2(~x, 0x00010001u); }
 /* 16-bit shared-memory accesses at a 32-bit shared address */
 __device__ __forceinline__ uint32_t lds16(uint32_t a)
 {
@@ -117,6 +118,7 @@ struct PairCheck {
     uint32_t live, inm, outm; /* bit 2k: owned slot k is a link / is read late / is written early */
     uint32_t n0, n1, p0, p1, idxh, sgn;
     uint32_t min0, min1, sg, mn0, mn1;
+    uint32_t m0p1, nmn0, nmn1; /* min0 + 1, -mn0, -mn1 (set by finish) */
 
     __device__ __forceinline__ void setup(const int2* __restrict__ ent, int cnt, int K, int q, int i, int j,
                                           int rr, uint2 rec, uint32_t fresh, unsigned long long meta,
@@ -153,8 +155,8 @@ struct PairCheck {
         /* minus the message: +m if it is negative, else -min(m, 31) */
         n0 = m0;
         n1 = m1;
-        p0 = neg2(__vmins2(m0, 0x001F001Fu));
-        p1 = neg2(__vmins2(m1, 0x001F001Fu));
+        p0 = __viaddmax_s16x2(~m0, 0x00010001u, 0xFFE1FFE1u); /* max(-m, -31) */
+        p1 = __viaddmax_s16x2(~m1, 0x00010001u, 0xFFE1FFE1u);
         min0 = min1 = 0x00FF00FFu;
         sg = 0;
     }
@@ -221,7 +223,7 @@ struct PairCheck {
         n0 = n1 = p0 = p1 = sgn = 0;
         idxh = 0x64006400u;
         min0 = min1 = 0x00FF00FFu;
-        sg = mn0 = mn1 = 0;
+        sg = mn0 = mn1 = m0p1 = nmn0 = nmn1 = 0;
     }
 
     /* the late slots (their bits were written by earlier levels) of a check
@@ -268,6 +270,9 @@ struct PairCheck {
             sg ^= bs;
             mn0 = m0;
             mn1 = m1;
+            m0p1 = __vadd2(c0, 0x00010001u);
+            nmn0 = neg2(m0);
+            nmn1 = neg2(m1);
         }
     }
 
@@ -277,9 +282,10 @@ struct PairCheck {
     __device__ __forceinline__ uint32_t update(int k, uint32_t& above, uint32_t& neg) const
     {
         const uint32_t v = x[k];
-        above = lmask(__viaddmin_s16x2(v, min0, __vsub2(min0, v))); /* min0 - |x| < 0 */
+        /* min0 - |x| = min(min0 + x, (min0 + 1) + ~x) < 0 */
+        above = lmask(__viaddmin_s16x2(~v, m0p1, __vadd2(min0, v)));
         neg = lmask(sg ^ v);
-        const uint32_t o = __vsub2(sel(above, mn0, mn1) ^ neg, neg);
+        const uint32_t o = sel(neg, sel(above, nmn0, nmn1), sel(above, mn0, mn1));
         return pk2(sadd(v, o));
     }
 
@@ -321,7 +327,7 @@ struct PairCheck {
             nidx = __vmaxs2(nidx, __shfl_xor_sync(gmask, nidx, 1));
             nsg |= __shfl_xor_sync(gmask, nsg, 1);
         }
-        nidx = __vmaxs2(__vsub2(nidx, 0x00010001u), 0u); /* slot number */
+        nidx = __viaddmax_s16x2(nidx, 0xFFFFFFFFu, 0u); /* slot number: max(nidx - 1, 0) */
         if (r == 0) {
             const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
             __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
@@ -420,13 +426,13 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
             const uint32_t pp = i ? sx2(post[c.K + kQCp * (i - 1) + j])
                                   : (j ? sx2(post[c.K + kQCp * (c.q - 1) + j - 1]) : 0x00010001u);
             uint32_t par = pc ^ pp;
-            uint32_t z = (__vsub2(pc, 0x00010001u) & ~pc) | (__vsub2(pp, 0x00010001u) & ~pp);
+            uint32_t z = (__vadd2(pc, 0xFFFFFFFFu) & ~pc) | (__vadd2(pp, 0xFFFFFFFFu) & ~pp);
             const int e1 = fr.eoff[i + 1];
             for (int e = fr.eoff[i]; e < e1; e++) {
                 const int2 en = fr.ent[e];
                 const uint32_t v = sx2(lds16((uint32_t)en.x + 2u * (uint32_t)j + (j < en.y ? 2u * kQCp : 0u)));
                 par ^= v;
-                z |= __vsub2(v, 0x00010001u) & ~v;
+                z |= __vadd2(v, 0xFFFFFFFFu) & ~v;
             }
             const uint32_t bad = (par | z);
             const int f = ((bad >> 15) & 1) | ((bad >> 30) & 2);

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dvbrx_b200.h"
@@ -312,8 +313,8 @@ bool ensure_pipe(drx_ldpc* d)
         return true;
     bool ok = cuda_ok(cudaStreamCreateWithFlags(&d->pipe[0], cudaStreamNonBlocking), "cudaStreamCreate") &&
               cuda_ok(cudaStreamCreateWithFlags(&d->pipe[1], cudaStreamNonBlocking), "cudaStreamCreate") &&
-              cuda_ok(cudaMalloc(&d->chunk_work, 16 * sizeof(unsigned)), "cudaMalloc");
-    for (int k = 0; ok && k < 16; k++)
+              cuda_ok(cudaMalloc(&d->chunk_work, kMaxChunks * sizeof(unsigned)), "cudaMalloc");
+    for (int k = 0; ok && k < kChunkEvents; k++)
         ok = cuda_ok(cudaEventCreateWithFlags(&d->chunk_ev[k], cudaEventDisableTiming), "cudaEventCreate");
     if (ok)
         ok = cuda_ok(cudaStreamCreateWithFlags(&d->copy, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -348,6 +349,40 @@ bool ensure_msg2(drx_ldpc* d, size_t need)
  * frame counter, the stream's own message slab), its results returned on
  * the same stream.  Copies of later chunks overlap earlier decodes, and the
  * CTAs of chunk c + 1 take the SMs that chunk c's tail leaves. */
+/* memcpy on up to 8 host threads for large copies (the staging copies of a
+ * host call run at the speed of one core otherwise) */
+void par_memcpy(void* dst, const void* src, size_t n)
+{
+    const size_t kMin = (size_t)4 << 20;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = (int)std::min<size_t>(std::min(8u, hw ? hw : 1u), n / kMin);
+    if (nt <= 1) {
+        memcpy(dst, src, n);
+        return;
+    }
+    const size_t part = (n / nt + 63) & ~(size_t)63;
+    std::vector<std::thread> th;
+    for (int k = 1; k < nt; k++) {
+        const size_t a = part * k;
+        if (a >= n)
+            break;
+        const size_t len = std::min(part, n - a);
+        th.emplace_back([=] { memcpy((char*)dst + a, (const char*)src + a, len); });
+    }
+    memcpy(dst, src, std::min(part, n));
+    for (auto& t : th)
+        t.join();
+}
+
+/*
+ * Host batch, pipelined: the batch goes in chunks, each staged into pinned
+ * memory on the host, copied in on the copy stream and decoded on one of two
+ * alternating streams (each with its own message slab), so that copies
+ * overlap decodes and a chunk's tail overlaps the next chunk.  The first
+ * chunk is one wave of the decoder (every CTA busy once), so that the GPU
+ * starts early; chunks then double.  Each chunk's results are copied back
+ * on its decode stream and out of pinned memory while later chunks decode.
+ */
 int decode_host_pipelined(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t* iters, uint8_t* ok, int nframes,
                           int max_iter)
 {
@@ -355,50 +390,77 @@ int decode_host_pipelined(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t*
     const size_t mb = launch_msg_bytes(d);
     if (!ensure_stage(d, nframes) || !ensure_pipe(d) || !ensure_scratch(d, mb) || !ensure_msg2(d, mb))
         return -1;
-    const int nch = std::min(8, nframes / 256);
-    const int per = ((nframes + nch - 1) / nch + 1) & ~1;
+    /* chunk sizes: one wave, then doubling, at most kMaxChunks chunks */
+    const int wave = use_pair(d) ? 2 * d->pair_ctas_per_sm * d->sms : d->ctas_per_sm * d->sms;
+    std::vector<int> first, size;
+    int f0 = 0, sz = std::max(2, wave & ~1);
+    while (f0 < nframes) {
+        const int left = kMaxChunks - (int)size.size();
+        int n = std::min(sz, nframes - f0);
+        if (left == 1)
+            n = nframes - f0;
+        else
+            n = std::max(n, std::min(nframes - f0, (nframes - f0 + left - 1) / left));
+        first.push_back(f0);
+        size.push_back(n);
+        f0 += n;
+        if (size.size() > 1)
+            sz *= 2;
+    }
+    const int nch = (int)size.size();
+    cudaEvent_t* in_ev = d->chunk_ev;
+    cudaEvent_t* out_ev = d->chunk_ev + kMaxChunks;
+    cudaEvent_t start = d->chunk_ev[2 * kMaxChunks];
     /* work queued on the handle's stream goes first (it may use the scratch) */
-    if (!cuda_ok(cudaEventRecord(d->chunk_ev[15], d->stream), "cudaEventRecord") ||
-        !cuda_ok(cudaStreamWaitEvent(d->copy, d->chunk_ev[15], 0), "cudaStreamWaitEvent") ||
-        !cuda_ok(cudaStreamWaitEvent(d->pipe[0], d->chunk_ev[15], 0), "cudaStreamWaitEvent") ||
-        !cuda_ok(cudaStreamWaitEvent(d->pipe[1], d->chunk_ev[15], 0), "cudaStreamWaitEvent"))
+    if (!cuda_ok(cudaEventRecord(start, d->stream), "cudaEventRecord") ||
+        !cuda_ok(cudaStreamWaitEvent(d->copy, start, 0), "cudaStreamWaitEvent") ||
+        !cuda_ok(cudaStreamWaitEvent(d->pipe[0], start, 0), "cudaStreamWaitEvent") ||
+        !cuda_ok(cudaStreamWaitEvent(d->pipe[1], start, 0), "cudaStreamWaitEvent"))
         return -1;
-    int rc = 0;
-    int c = 0;
-    for (size_t f0 = 0; f0 < (size_t)nframes && rc == 0; f0 += per, c++) {
-        const int n = (int)std::min((size_t)per, (size_t)nframes - f0);
-        memcpy(d->h_llr + f0 * N, llr + f0 * N, (size_t)n * N);
+    int rc = 0, queued = 0;
+    for (int c = 0; c < nch && rc == 0; c++, queued++) {
+        const size_t a = (size_t)first[c];
+        const int n = size[c];
+        par_memcpy(d->h_llr + a * N, llr + a * N, (size_t)n * N);
         cudaStream_t ks = d->pipe[c & 1];
         Extra x;
         x.work = d->chunk_work + c;
         x.msg = (c & 1) ? d->msg2 : d->msg;
-        if (!cuda_ok(cudaMemcpyAsync(d->d_llr + f0 * N, d->h_llr + f0 * N, (size_t)n * N, cudaMemcpyHostToDevice,
+        if (!cuda_ok(cudaMemcpyAsync(d->d_llr + a * N, d->h_llr + a * N, (size_t)n * N, cudaMemcpyHostToDevice,
                                      d->copy),
                      "cudaMemcpyAsync") ||
-            !cuda_ok(cudaEventRecord(d->chunk_ev[c], d->copy), "cudaEventRecord") ||
-            !cuda_ok(cudaStreamWaitEvent(ks, d->chunk_ev[c], 0), "cudaStreamWaitEvent") ||
-            enqueue(d, d->d_llr + f0 * N, N, d->d_out + f0 * nb, nb, d->d_it + f0, d->d_ok + f0, n, max_iter, 0, ks,
+            !cuda_ok(cudaEventRecord(in_ev[c], d->copy), "cudaEventRecord") ||
+            !cuda_ok(cudaStreamWaitEvent(ks, in_ev[c], 0), "cudaStreamWaitEvent") ||
+            enqueue(d, d->d_llr + a * N, N, d->d_out + a * nb, nb, d->d_it + a, d->d_ok + a, n, max_iter, 0, ks,
                     &x) ||
-            !cuda_ok(cudaMemcpyAsync(d->h_out + f0 * nb, d->d_out + f0 * nb, (size_t)n * nb, cudaMemcpyDeviceToHost,
+            !cuda_ok(cudaMemcpyAsync(d->h_out + a * nb, d->d_out + a * nb, (size_t)n * nb, cudaMemcpyDeviceToHost,
                                      ks),
                      "cudaMemcpyAsync") ||
-            !cuda_ok(cudaMemcpyAsync(d->h_it + f0, d->d_it + f0, (size_t)n * 4, cudaMemcpyDeviceToHost, ks),
+            !cuda_ok(cudaMemcpyAsync(d->h_it + a, d->d_it + a, (size_t)n * 4, cudaMemcpyDeviceToHost, ks),
                      "cudaMemcpyAsync") ||
-            !cuda_ok(cudaMemcpyAsync(d->h_ok + f0, d->d_ok + f0, (size_t)n, cudaMemcpyDeviceToHost, ks),
-                     "cudaMemcpyAsync"))
+            !cuda_ok(cudaMemcpyAsync(d->h_ok + a, d->d_ok + a, (size_t)n, cudaMemcpyDeviceToHost, ks),
+                     "cudaMemcpyAsync") ||
+            !cuda_ok(cudaEventRecord(out_ev[c], ks), "cudaEventRecord"))
             rc = -1;
+    }
+    /* results out of pinned memory, chunk by chunk, as they arrive */
+    for (int c = 0; c < queued && rc == 0; c++) {
+        if (!cuda_ok(cudaEventSynchronize(out_ev[c]), "decode")) {
+            rc = -1;
+            break;
+        }
+        const size_t a = (size_t)first[c];
+        const int n = size[c];
+        par_memcpy(out + a * nb, d->h_out + a * nb, (size_t)n * nb);
+        if (iters)
+            memcpy(iters + a, d->h_it + a, (size_t)n * 4);
+        if (ok)
+            memcpy(ok + a, d->h_ok + a, (size_t)n);
     }
     const bool s0 = cuda_ok(cudaStreamSynchronize(d->pipe[0]), "decode");
     const bool s1 = cuda_ok(cudaStreamSynchronize(d->pipe[1]), "decode");
     const bool s2 = cuda_ok(cudaStreamSynchronize(d->copy), "copy");
-    if (rc || !s0 || !s1 || !s2)
-        return -1;
-    memcpy(out, d->h_out, (size_t)nframes * nb);
-    if (iters)
-        memcpy(iters, d->h_it, (size_t)nframes * 4);
-    if (ok)
-        memcpy(ok, d->h_ok, (size_t)nframes);
-    return 0;
+    return rc || !s0 || !s1 || !s2 ? -1 : 0;
 }
 
 bool ensure_fallback(drx_ldpc* d, size_t nframes)
@@ -503,7 +565,7 @@ void drx_ldpc_free(drx_ldpc* d)
     cudaFree(d->msg);
     cudaFree(d->msg2);
     cudaFree(d->chunk_work);
-    for (int k = 0; k < 16; k++)
+    for (int k = 0; k < kChunkEvents; k++)
         if (d->chunk_ev[k])
             cudaEventDestroy(d->chunk_ev[k]);
     for (int k = 0; k < 2; k++)

@@ -14,6 +14,10 @@
 using drxg::Code;
 using drxg::DevCode;
 
+/* chunks of a pipelined host call, and their events (two per chunk + one) */
+constexpr int kMaxChunks = 15;
+constexpr int kChunkEvents = 2 * kMaxChunks + 1;
+
 struct drx_ldpc {
     int device = 0;
     int sms = 0;
@@ -49,7 +53,7 @@ struct drx_ldpc {
      * events and frame counters, and a second message slab */
     cudaStream_t pipe[2] = {nullptr, nullptr};
     cudaStream_t copy = nullptr;
-    cudaEvent_t chunk_ev[16] = {};
+    cudaEvent_t chunk_ev[kChunkEvents] = {}; /* per chunk: copied in, results out; then the start */
     unsigned* chunk_work = nullptr;
     void* msg2 = nullptr;
     size_t msg2_cap = 0;

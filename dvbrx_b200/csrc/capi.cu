@@ -253,7 +253,7 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
         p.work = work;
         if (!cuda_ok(cudaMemsetAsync(work, 0, sizeof(unsigned), s), "cudaMemsetAsync"))
             return -1;
-        const size_t slab = decode_pair_msg_bytes(d->code.R);
+        const size_t slab = decode_pair_msg_bytes(d->code.R, d->pair_kid);
         if (!(x && x->msg) && !ensure_scratch(d, slab * (size_t)grid))
             return -1;
         p.msg = x && x->msg ? x->msg : d->msg;
@@ -326,7 +326,7 @@ size_t launch_msg_bytes(const drx_ldpc* d)
 {
     size_t a = decode_msg_bytes(d->code.R, d->code.dclass) * (size_t)(d->ctas_per_sm * d->sms);
     if (d->pair_ctas_per_sm > 0)
-        a = std::max(a, decode_pair_msg_bytes(d->code.R) * (size_t)(d->pair_ctas_per_sm * d->sms));
+        a = std::max(a, decode_pair_msg_bytes(d->code.R, d->pair_kid) * (size_t)(d->pair_ctas_per_sm * d->sms));
     return a;
 }
 

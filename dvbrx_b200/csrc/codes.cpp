@@ -128,6 +128,7 @@ bool compile_code(int table, Code* c, std::string* err)
     c->nlev.assign(q, 1);
     c->lmeta.assign((size_t)q * QC, 0);
     c->levelled = false;
+    c->phased = true;
     c->nlevels = 0;
     for (int i = 0; i < q; i++) {
         /* per check j: which of its information slots share their bit with
@@ -146,10 +147,13 @@ bool compile_code(int table, Code* c, std::string* err)
                     else if (jp > j)
                         out |= 1ull << (2 + x);
                 }
-            /* masks of 24 slots: layers with more links (check degree
-             * above 24) keep none; the phased schedule does not run them */
-            if (2 + ne <= 24)
+            /* masks of 24 slots: the shared links come first, so only a
+             * layer with more than 22 of them would need more (it keeps
+             * none, and the phased schedule does not run it) */
+            if (((in | out) >> 24) == 0)
                 c->lmeta[(size_t)i * QC + j] = in << 8 | out << 32;
+            else
+                c->phased = false;
         }
         std::vector<int> offs; /* d: check j shares a bit with check (j + d) mod 360 */
         for (size_t x = 0; x < layer[i].size(); x++)

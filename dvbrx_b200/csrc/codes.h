@@ -39,6 +39,7 @@ struct Code {
     int edges = 0;     /* links of the whole Tanner graph */
     int nlevels = 0;   /* steps per iteration */
     bool levelled = false;
+    bool phased = true; /* lmeta holds every check's late and early slots */
     /* per layer i: entries eoff[i] .. eoff[i+1]-1, each a pair
      * (360*g - a, a): check j of the layer links information bit
      * 360*g - a + j, plus 360 if j < a */

@@ -139,12 +139,12 @@ cudaError_t launch_decode(const DecodeParams& p, int dclass, size_t smem, int gr
 namespace drxg {
 
 /* Frame-pair variant (ldpc_pair.cu): two frames per CTA in 16x2 SIMD, codes
- * up to check degree 14; per-frame stopping only.  pair_kernel_id picks the
+ * up to check degree 32; per-frame stopping only.  pair_kernel_id picks the
  * instantiation for a code (-1: not run by the frame-pair kernel). */
 struct Code;
 int pair_kernel_id(const Code& c);
 size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q);
-size_t decode_pair_msg_bytes(int R);
+size_t decode_pair_msg_bytes(int R, int kid);
 int decode_pair_ctas_per_sm(int kid, size_t smem);
 cudaError_t launch_decode_pair(const DecodeParams& p, int kid, size_t smem, int grid, cudaStream_t stream);
 

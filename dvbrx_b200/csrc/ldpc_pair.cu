@@ -29,7 +29,8 @@
  * passes the syndrome check or reaches max_iter, its results are written
  * and the lane takes the next frame of the batch (its first iteration reads
  * zero messages), so a converged frame never waits for its neighbour.
- * Codes up to check degree 14 (degree classes 0-2) run here.
+ * Every DVB-S2, S2X and T2 code runs here (check degrees up to 30; message
+ * records of 16 bytes above degree 16).
  */
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -46,7 +47,7 @@ constexpr int kQCp = 360;
 /* a kernel compiled for LS late slots reads late and writes early only owned
  * slots 1 .. LS of each thread (link slots 2 .. 2 LS + 1); two cover every
  * pair code but short 3/5 and 4/5, which take three */
-constexpr int kLateSlotsMax = 3;
+constexpr int kLateSlotsMax = 6;
 
 /* PRMT in its default mode: a selector nibble with bit 3 set replicates the
  * sign bit of the selected byte.  (__byte_perm keeps only the low 3 bits of
@@ -106,8 +107,19 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
  * in its level), enters the minimums as 255, which no magnitude reaches;
  * stores are predicated.
  */
-template <int DM, bool EXACT, int LS, int T>
+/* A check's message record: 8 bytes up to degree 16 (per lane min0, min1
+ * and a 4-bit index in one word, 16 sign bits per lane in the other); 16
+ * bytes above (min0 and min1; sign bits of slots 0-15 and of slots 16-31;
+ * the index, 16 bits per lane). */
+template <bool WIDE>
+using PairRec = typename std::conditional<WIDE, uint4, uint2>::type;
+
+/* WIDE: the kernel's records are 16 bytes (its degree bound is above 16) */
+template <int DM, bool EXACT, int LS, int T, bool WIDE>
 struct PairCheck {
+    static_assert(!WIDE || T == 1, "records of more than 16 links are built by one thread");
+    static_assert(DM <= (WIDE ? 32 : 16), "degree above the record's slots");
+    using Rec = PairRec<WIDE>;
     static constexpr int S = T == 2 ? (DM + 1) / 2 : DM;
     /* owned slots that can be late or early: k0 .. k1 (link slots 2 .. 2 LS + 1) */
     static constexpr int K0 = T == 2 ? 1 : 2;
@@ -116,12 +128,12 @@ struct PairCheck {
     uint32_t addr[S]; /* shared-memory byte addresses of the owned links' posteriors */
     uint32_t x[S];
     uint32_t live, inm, outm; /* bit 2k: owned slot k is a link / is read late / is written early */
-    uint32_t n0, n1, p0, p1, idxh, sgn;
+    uint32_t n0, n1, p0, p1, idxh, sgn, sgn1; /* sgn: sign bits of slots 0-15, sgn1: 16-31 */
     uint32_t min0, min1, sg, mn0, mn1;
     uint32_t m0p1, nmn0, nmn1; /* min0 + 1, -mn0, -mn1 (set by finish) */
 
     __device__ __forceinline__ void setup(const int2* __restrict__ ent, int cnt, int K, int q, int i, int j,
-                                          int rr, uint2 rec, uint32_t fresh, unsigned long long meta,
+                                          int rr, Rec rec, uint32_t fresh, unsigned long long meta,
                                           uint32_t sbase)
     {
         r = rr;
@@ -151,7 +163,13 @@ struct PairCheck {
         const uint32_t w0 = rec.x & ~fresh;
         sgn = (rec.y & ~fresh) >> r;
         const uint32_t m0 = w0 & 0x003F003Fu, m1 = (w0 >> 6) & 0x003F003Fu;
-        idxh = (((w0 >> 12) & 0x000F000Fu) | 0x64006400u) - (uint32_t)r * 0x00010001u; /* FP16 1024 + index - r */
+        if constexpr (WIDE) {
+            sgn1 = rec.z & ~fresh;
+            idxh = (rec.w & ~fresh) | 0x64006400u; /* FP16 1024 + index */
+        } else {
+            sgn1 = 0;
+            idxh = (((w0 >> 12) & 0x000F000Fu) | 0x64006400u) - (uint32_t)r * 0x00010001u; /* FP16 1024 + index - r */
+        }
         /* minus the message: +m if it is negative, else -min(m, 31) */
         n0 = m0;
         n1 = m1;
@@ -165,7 +183,7 @@ struct PairCheck {
     __device__ __forceinline__ uint32_t unmsg(int k) const
     {
         const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(T * k) * 0x00010001u);
-        const uint32_t sm = lmask(sgn << (15 - T * k));
+        const uint32_t sm = lmask((T * k < 16 ? sgn : sgn1) << (15 - ((T * k) & 15)));
         return sel(sm, sel(im, n1, n0), sel(im, p1, p0));
     }
 
@@ -220,7 +238,7 @@ struct PairCheck {
             x[k] = 0x00FF00FFu;
         }
         live = inm = outm = 0;
-        n0 = n1 = p0 = p1 = sgn = 0;
+        n0 = n1 = p0 = p1 = sgn = sgn1 = 0;
         idxh = 0x64006400u;
         min0 = min1 = 0x00FF00FFu;
         sg = mn0 = mn1 = m0p1 = nmn0 = nmn1 = 0;
@@ -307,10 +325,10 @@ struct PairCheck {
     /* every other posterior (predicated stores) and the node's compressed
      * messages for both lanes, stored by thread 0: the slot holding min0 and
      * one sign bit per slot */
-    __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, unsigned gmask, uint2* __restrict__ dst)
+    __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, unsigned gmask, Rec* __restrict__ dst)
     {
         const uint32_t wm = live & ~outm;
-        uint32_t nidx = 0, nsg = 0; /* nidx per lane: T k + 1 of an owned slot holding min0, 0 if none */
+        uint32_t nidx = 0, nsg = 0, nsg1 = 0; /* nidx per lane: T k + 1 of an owned slot holding min0, 0 if none */
 #pragma unroll
         for (int k = 0; k < S; k++) {
             uint32_t above, neg;
@@ -318,7 +336,10 @@ struct PairCheck {
             if ((wm >> (T * k)) & 1u)
                 sts16(addr[k], nv);
             nidx = sel(above, nidx, (uint32_t)(T * k + 1) * 0x00010001u);
-            nsg |= neg & (0x00010001u << (T * k));
+            if (T * k < 16)
+                nsg |= neg & (0x00010001u << (T * k));
+            else
+                nsg1 |= neg & (0x00010001u << (T * k - 16));
         }
         if (T == 2) {
             nsg <<= r; /* bit 2k -> slot 2k + r (slots stay below 16: no carry across lanes) */
@@ -330,7 +351,10 @@ struct PairCheck {
         nidx = __viaddmax_s16x2(nidx, 0xFFFFFFFFu, 0u); /* slot number: max(nidx - 1, 0) */
         if (r == 0) {
             const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
-            __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
+            if constexpr (WIDE)
+                __stcg(dst, make_uint4(m0c | (m1c << 6), nsg, nsg1, nidx));
+            else
+                __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
         }
     }
 };
@@ -458,9 +482,10 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
  * constrain the bits two checks of a layer share, so the wavefront levels
  * carry just those links.  Unlevelled layers take one pass.
  */
-template <int DM, bool EXACT, int LS, int T, bool LEARNED>
-__device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev, uint2 rec,
-                                           unsigned long long meta, uint32_t fresh, uint2* __restrict__ msg,
+template <int DM, bool EXACT, int LS, int T, bool WIDE, bool LEARNED>
+__device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev,
+                                           PairRec<WIDE> rec, unsigned long long meta, uint32_t fresh,
+                                           PairRec<WIDE>* __restrict__ msg,
                                            int lA, int lB)
 {
     const int t = threadIdx.x;
@@ -475,7 +500,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             b = s_learn_tab[lB + k];
         }
     };
-    PairCheck<DM, EXACT, LS, T> ck;
+    PairCheck<DM, EXACT, LS, T, WIDE> ck;
     if (active) {
         ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, T == 2 ? t & 1 : 0, rec, fresh, meta,
                  (uint32_t)__cvta_generic_to_shared(fr.post));
@@ -507,7 +532,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
                 __syncthreads();
             }
         };
-        using Ck = PairCheck<DM, EXACT, LS, T>;
+        using Ck = PairCheck<DM, EXACT, LS, T, WIDE>;
         constexpr int KS = T == 1 && Ck::K1 > 3 ? 3 : Ck::K1;
         const uint32_t lm = __reduce_or_sync(0xFFFFFFFFu, ck.inm | ck.outm);
         if (KS < Ck::K1 && (lm >> (T * (KS + 1))) != 0)
@@ -533,20 +558,22 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
  * the two information-link counts A <= B of its codes (exact-degree check
  * nodes), or, with GDM > 0, for any count up to GDM - 2 (predicated). */
 template <int A, int B, int GDM, int LS, int T, bool LEARNED>
-__device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __restrict__ msg, uint32_t fresh,
-                             int lA, int lB)
+__device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, uint32_t fresh, int lA, int lB)
 {
+    constexpr bool WIDE = (GDM > 0 ? GDM : B + 2) > 16;
+    using Rec = PairRec<WIDE>;
+    Rec* __restrict__ msg = (Rec*)msgv;
     const int t = threadIdx.x;
     const int j = T == 2 ? t >> 1 : t;
     const bool active = t < T * kQCp;
-    uint2 rn = make_uint2(0, 0);
+    Rec rn{};
     unsigned long long mn = 0;
     if (active) {
         rn = __ldcg(msg + j);
         mn = __ldg(c.lmeta + j);
     }
     for (int i = 0; i < c.q; i++) {
-        const uint2 rec = rn;
+        const Rec rec = rn;
         const unsigned long long meta = mn;
         if (active && i + 1 < c.q) {
             rn = __ldcg(msg + kQCp * (i + 1) + j);
@@ -555,11 +582,11 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, uint2* __res
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
         const int nlev = c.nlev[i];
         if (GDM > 0)
-            layer_pair<(GDM > 0 ? GDM : 2), false, LS, T, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<(GDM > 0 ? GDM : 2), false, LS, T, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else if (A == B || cnt == A)
-            layer_pair<A + 2, true, LS, T, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<A + 2, true, LS, T, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else
-            layer_pair<B + 2, true, LS, T, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<B + 2, true, LS, T, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
     }
 }
 
@@ -587,7 +614,7 @@ __global__ void __launch_bounds__(T * 384, 1) k_decode_pair(DecodeParams p)
     const PairFrame fr = stage_pair(c, smem);
     const int lT = stage_learn(p.learn, p.learn_class, p.learn_iters);
     const int nframes = p.nframes_dev ? *p.nframes_dev : p.nframes;
-    uint2* msg = (uint2*)((char*)p.msg + (size_t)blockIdx.x * p.msg_stride);
+    void* msg = (char*)p.msg + (size_t)blockIdx.x * p.msg_stride;
     const int t = threadIdx.x;
     if (t == 0) {
         s_frame[0] = s_frame[1] = -1;
@@ -667,33 +694,52 @@ size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q)
            a16(sizeof(uint32_t) * nsteps);
 }
 
-size_t decode_pair_msg_bytes(int R) { return (size_t)R * sizeof(uint2); }
 
 /* Pair kernels by information-link counts (A, B): every pair of the DVB-S2,
- * S2X and T2 codes up to check degree 14, plus predicated kernels for the
- * codes whose layers have more than two different counts. */
+ * S2X and T2 codes, plus predicated kernels for the codes whose layers have
+ * more than two different counts (degree bounds 7, 11, 14, 22, 32).  LS:
+ * late slots the kernel carries (two cover most levelled codes; normal 4/5
+ * and 9/10 need four, short 5/6 five, short 8/9 six). */
 struct PairKernel {
     int a, b, gdm, ls, threads;
     const void* fn;
 };
 
-#define DRXG_PK(a, b) { a, b, 0, 2, 384, (const void*)k_decode_pair<a, b, 0, 2, 1> }
-#define DRXG_PK3(a, b) { a, b, 0, 3, 384, (const void*)k_decode_pair<a, b, 0, 3, 1> }
-#define DRXG_PG(d) { 0, 0, d, 3, 384, (const void*)k_decode_pair<1, 1, d, 3, 1> }
+#define DRXG_PKL(a, b, ls) { a, b, 0, ls, 384, (const void*)k_decode_pair<a, b, 0, ls, 1> }
+#define DRXG_PK(a, b) DRXG_PKL(a, b, 2)
+#define DRXG_PK3(a, b) DRXG_PKL(a, b, 3)
+#define DRXG_PGL(d, ls) { 0, 0, d, ls, 384, (const void*)k_decode_pair<1, 1, d, ls, 1> }
+#define DRXG_PG(d) DRXG_PGL(d, 3)
 static const PairKernel kPairKernels[] = {
     DRXG_PK(1, 2), DRXG_PK(2, 2), DRXG_PK(2, 3), DRXG_PK(3, 3), DRXG_PK(4, 4), DRXG_PK(5, 5),
     DRXG_PK(5, 6), DRXG_PK(6, 7), DRXG_PK(7, 7), DRXG_PK(7, 8), DRXG_PK(8, 8), DRXG_PK(8, 9),
     DRXG_PK(9, 9), DRXG_PK(9, 10), DRXG_PK(11, 11), DRXG_PK(11, 12), DRXG_PK(12, 12), DRXG_PK3(9, 9),
-    DRXG_PG(7), DRXG_PG(11), DRXG_PG(14),
+    DRXG_PK(12, 13), DRXG_PK(13, 14),
+    /* check degrees above 16: 16-byte message records */
+    DRXG_PK(14, 15), DRXG_PKL(16, 16, 4), DRXG_PK(17, 18), DRXG_PK3(20, 20), DRXG_PKL(25, 25, 6), DRXG_PK(27, 28),
+    DRXG_PKL(28, 28, 4),
+    DRXG_PG(7), DRXG_PG(11), DRXG_PG(14), DRXG_PGL(22, 5), DRXG_PGL(32, 6),
 };
+#undef DRXG_PKL
 #undef DRXG_PK
 #undef DRXG_PK3
+#undef DRXG_PGL
 #undef DRXG_PG
 constexpr int kNumPairKernels = (int)(sizeof(kPairKernels) / sizeof(kPairKernels[0]));
 
+/* message slab of one CTA: one record per check, 8 or 16 bytes */
+size_t decode_pair_msg_bytes(int R, int kid)
+{
+    if (kid < 0 || kid >= kNumPairKernels)
+        return 0;
+    const PairKernel& k = kPairKernels[kid];
+    const int dm = k.gdm > 0 ? k.gdm : k.b + 2;
+    return (size_t)R * (dm > 16 ? sizeof(uint4) : sizeof(uint2));
+}
+
 int pair_kernel_id(const Code& c)
 {
-    if (c.deg_max > 14)
+    if (c.deg_max > 32 || !c.phased)
         return -1;
     /* late slots the code needs: link slots 2 .. 2 ls + 1 */
     int ls = 0;

@@ -298,7 +298,7 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
             continue;
         drx_ldpc* h = m->codes[c];
         const bool pair = pair_runs(h);
-        code_slab[c] = pair ? decode_pair_msg_bytes(h->code.R) : decode_msg_bytes(h->code.R, h->code.dclass);
+        code_slab[c] = pair ? decode_pair_msg_bytes(h->code.R, h->pair_kid) : decode_msg_bytes(h->code.R, h->code.dclass);
         code_grid[c] = pair ? std::min((count[c] + 1) / 2, h->pair_ctas_per_sm * h->sms)
                             : std::min(count[c], h->ctas_per_sm * h->sms);
         code_side[c] = k;

@@ -137,9 +137,9 @@ int drx_channel_generate(drx_ldpc* d, const char* constellation, const char* con
                          void* stream);
 
 /* Kernel of the per-frame batch calls: DRX_VARIANT_AUTO (the default) runs
- * the frame-pair kernel (two frames per CTA, 16x2 SIMD) for codes up to
- * check degree 14 and the one-frame kernel otherwise; DRX_VARIANT_FRAME
- * pins the one-frame kernel.  Both give identical results.  Returns the
+ * the frame-pair kernel (two frames per CTA, 16x2 SIMD), which covers every
+ * code; DRX_VARIANT_FRAME pins the one-frame kernel.  Both give identical
+ * results.  Returns the
  * variant per-frame batches will now run (DRX_VARIANT_FRAME or
  * DRX_VARIANT_PAIR), or -1. */
 #define DRX_VARIANT_AUTO 0

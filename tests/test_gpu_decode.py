@@ -199,12 +199,14 @@ def test_kernel_variants_agree(short, rate, const, es, n, max_iter):
 
 
 def test_variant_auto_choice():
-    d = handle(0, "3_5")
-    assert d.set_variant(D.VARIANT_AUTO) == D.VARIANT_PAIR
-    hi = handle(0, "9_10")  # check degree 30: one-frame kernel only
-    assert hi.set_variant(D.VARIANT_AUTO) == D.VARIANT_FRAME
-    with pytest.raises(ValueError):
-        hi.set_variant(D.VARIANT_PAIR)
+    """Every code, up to check degree 30 (normal 9/10), runs on the frame-pair
+    kernel by default; the one-frame kernel can still be chosen."""
+    for short, rate in ((0, "3_5"), (0, "9_10"), (1, "8_9"), (0, "2_3_t2")):
+        d = handle(short, rate)
+        assert d.set_variant(D.VARIANT_AUTO) == D.VARIANT_PAIR, rate
+        assert d.set_variant(D.VARIANT_FRAME) == D.VARIANT_FRAME
+        assert d.set_variant(D.VARIANT_PAIR) == D.VARIANT_PAIR
+        d.set_variant(D.VARIANT_AUTO)
 
 
 @pytest.mark.parametrize("short,rate,n", [(1, "1_2", 1500), (0, "3_5", 777), (0, "9_10", 600)])

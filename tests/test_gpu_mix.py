@@ -14,8 +14,8 @@ CODES = [
     (0, "3_5", "8PSK", 6.0),
     (0, "2_3", "8PSK", 6.8),
     (1, "1_2", "QPSK", 1.6),
-    (0, "9_10", "QPSK", 7.0),   # degree 30: one-frame kernel only
-    (1, "8_9", "QPSK", 6.9),    # degree 27
+    (0, "9_10", "QPSK", 7.0),   # degree 30: 16-byte message records
+    (1, "8_9", "QPSK", 6.9),    # degree 27, shared links up to slot 13
     (0, "13_45", "QPSK", -0.6),
     (1, "11_45", "QPSK", 0.2),
 ]

@@ -229,7 +229,9 @@ namespace {
 /* Plan (capture) both tilings of a mixed batch.  learned: the first pass
  * runs every code's learned table for at most max_iter iterations, then the
  * failing rows are gathered on the device and decoded again by the plain
- * decoder (one launch, at most plain_max_iter iterations; none if <= 0). */
+ * decoder (at most plain_max_iter iterations; none if <= 0): in one launch
+ * for the one-launch tiling, per code right after its learned pass for the
+ * per-code tiling. */
 int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* llr, size_t llr_stride,
              uint8_t* out, size_t out_stride, int32_t* iters, uint8_t* ok, int max_iter, bool learned,
              int plain_max_iter, uint8_t* fallback)
@@ -317,7 +319,7 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
     total = std::max(total, mix_slab * (size_t)mix_grid);
     if (!cuda_check(cudaMalloc(&m->d_frame_code, sizeof(int32_t) * nframes), "cudaMalloc") ||
         !cuda_check(cudaMalloc(&m->d_order, sizeof(int32_t) * nframes), "cudaMalloc") ||
-        !cuda_check(cudaMalloc(&m->d_work, sizeof(unsigned) * (ncodes + 1)), "cudaMalloc") ||
+        !cuda_check(cudaMalloc(&m->d_work, sizeof(unsigned) * (2 * ncodes + 1)), "cudaMalloc") ||
         !cuda_check(cudaMalloc(&m->d_msg, total), "cudaMalloc") ||
         !cuda_check(cudaMemcpy(m->d_frame_code, code, sizeof(int32_t) * nframes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
         !cuda_check(cudaMemcpy(m->d_order, order.data(), sizeof(int32_t) * nframes, cudaMemcpyHostToDevice), "cudaMemcpy")) {
@@ -339,7 +341,7 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
         if (!cuda_check(cudaMalloc(&m->d_learn, sizeof(void*) * ncodes), "cudaMalloc") ||
             !cuda_check(cudaMalloc(&m->d_learn_cls, sizeof(void*) * ncodes), "cudaMalloc") ||
             !cuda_check(cudaMalloc(&m->d_learn_iters, sizeof(int) * ncodes), "cudaMalloc") ||
-            !cuda_check(cudaMalloc(&m->d_fb_rows, sizeof(int32_t) * (nframes + 4)), "cudaMalloc") ||
+            !cuda_check(cudaMalloc(&m->d_fb_rows, sizeof(int32_t) * (nframes + 4 + ncodes)), "cudaMalloc") ||
             !cuda_check(cudaMalloc(&m->d_fb_ok, nframes), "cudaMalloc") ||
             !cuda_check(cudaMemcpy(m->d_learn, lt.data(), sizeof(void*) * ncodes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
             !cuda_check(cudaMemcpy(m->d_learn_cls, lc.data(), sizeof(void*) * ncodes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
@@ -424,6 +426,28 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
                 if (e == cudaSuccess)
                     e = pair_runs(h) ? launch_decode_pair(p, h->pair_kid, h->pair_smem, code_grid[c], s)
                                      : launch_decode(p, h->code.dclass, h->smem, code_grid[c], s);
+                if (learned && e == cudaSuccess) {
+                    /* fallback of this code, on its stream: its failing rows through its own
+                     * plain kernel (the count read on the device) */
+                    int* cnt = (int*)(m->d_fb_rows + nframes + 4) + c;
+                    k_compact_failing<<<1, kCompactThreads, 0, s>>>(m->d_order + start[c], ok, count[c],
+                                                                    m->d_fb_rows + start[c], cnt, fallback);
+                    e = cudaGetLastError();
+                    if (e == cudaSuccess && plain_max_iter > 0) {
+                        DecodeParams q = p;
+                        q.learn = nullptr;
+                        q.learn_class = nullptr;
+                        q.learn_iters = 0;
+                        q.rows = m->d_fb_rows + start[c];
+                        q.nframes_dev = cnt;
+                        q.max_iter = plain_max_iter;
+                        q.work = m->d_work + ncodes + 1 + c;
+                        e = cudaMemsetAsync(q.work, 0, sizeof(unsigned), s);
+                        if (e == cudaSuccess)
+                            e = pair_runs(h) ? launch_decode_pair(q, h->pair_kid, h->pair_smem, code_grid[c], s)
+                                             : launch_decode(q, h->code.dclass, h->smem, code_grid[c], s);
+                    }
+                }
             }
             for (int s = 0; s < kSideStreams; s++) {
                 if (e == cudaSuccess)
@@ -432,7 +456,7 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
                     e = cudaStreamWaitEvent(m->capture, m->join[s], 0);
             }
         }
-        if (learned && e == cudaSuccess) {
+        if (learned && t == DRX_TILING_ONE_LAUNCH && e == cudaSuccess) {
             /* fallback: the failing rows, in processing order, through the plain one-launch kernel */
             int* cnt = (int*)(m->d_fb_rows + nframes);
             k_compact_failing<<<1, kCompactThreads, 0, m->capture>>>(m->d_order, ok, nframes, m->d_fb_rows, cnt,

@@ -183,6 +183,13 @@ def test_device_batch_strided():
     (0, "1_4", "QPSK", -1.0, 5, 30),
     (1, "8_15", "QPSK", 2.4, 31, 30),
     (0, "3_5", "8PSK", 6.0, 3, 0),
+    # check degrees above 16: 16-byte message records, four to six late slots
+    (0, "4_5", "QPSK", 4.9, 7, 30),
+    (0, "5_6", "QPSK", 5.4, 7, 30),
+    (0, "8_9", "QPSK", 6.4, 5, 30),
+    (0, "9_10", "QPSK", 6.6, 5, 30),
+    (1, "5_6", "QPSK", 5.5, 13, 30),
+    (1, "8_9", "QPSK", 6.6, 13, 30),
 ])
 def test_kernel_variants_agree(short, rate, const, es, n, max_iter):
     """The one-frame kernel and the frame-pair kernel (odd frame counts leave
@@ -223,3 +230,27 @@ def test_host_call_pipelined_matches_device(short, rate, n):
     assert np.array_equal(bits, tb.cpu().numpy())
     assert np.array_equal(it, ti.cpu().numpy())
     assert np.array_equal(ok, to.cpu().numpy())
+
+
+@pytest.mark.parametrize("short,rate,es,crate", [(0, "4_5", 4.7, None), (0, "5_6", 5.2, None), (0, "8_9", 6.2, None),
+                                                 (0, "9_10", 6.45, None), (1, "5_6", 5.3, None),
+                                                 (1, "8_9", 6.3, None), (0, "154_180", 5.6, "8_9"),
+                                                 (0, "135_180", 4.6, "3_4")])
+def test_pair_matches_frame_high_degree(short, rate, es, crate):
+    """Above check degree 16 the frame-pair kernel keeps 16-byte message
+    records and carries up to six late slots: on a few hundred frames around
+    the waterfall it gives the one-frame kernel's bits, iterations and flags."""
+    import torch
+
+    d = D.Ldpc(D.fec_lookup(short, rate), rate)
+    llr, _, _ = d.generate(300, es, seed=zlib.crc32(rate.encode()) + short, const_rate=crate)
+    out = {}
+    for v in (D.VARIANT_FRAME, D.VARIANT_PAIR):
+        assert d.set_variant(v) == v
+        out[v] = [t.cpu().numpy() for t in d.decode_device(llr, 30)]
+    torch.cuda.synchronize()
+    for a, b in zip(out[D.VARIANT_FRAME], out[D.VARIANT_PAIR]):
+        assert np.array_equal(a, b), rate
+    it, ok = out[D.VARIANT_PAIR][1], out[D.VARIANT_PAIR][2]
+    assert 0 < ok.sum() and it.max() > 3, "the case should have converging frames that need iterations"
+    d.close()

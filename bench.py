@@ -629,13 +629,17 @@ def run_b200(args):
     e2e = None
     if args.e2e_steps > 0:
         host = [l.cpu().numpy() for l in llr]
+        # output buffers allocated once and reused, as a receiver decoding batch after batch does
+        h_out = np.zeros((F, dec.nbytes), np.uint8)
+        h_it = np.zeros(F, np.int32)
+        h_ok = np.zeros(F, np.uint8)
         for k in range(min(2, args.e2e_steps)):
-            dec.decode_host(host[k % len(host)], MAX_ITER)
+            dec.decode_host(host[k % len(host)], MAX_ITER, out=h_out, iters=h_it, ok=h_ok)
         if world > 1:
             dist.barrier()
         t0 = time.perf_counter()
         for k in range(args.e2e_steps):
-            dec.decode_host(host[k % len(host)], MAX_ITER)
+            dec.decode_host(host[k % len(host)], MAX_ITER, out=h_out, iters=h_it, ok=h_ok)
         dt = max_over_ranks(time.perf_counter() - t0, world, "cuda")
         e2e = {"value": aggregate_gbps(world, args.e2e_steps * F, kldpc, dt * 1e3), "unit": UNIT,
                "h2d_bytes_per_step": F * dec.N,

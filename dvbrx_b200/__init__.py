@@ -211,13 +211,18 @@ class Ldpc:
             assert r.dtype == np.uint8 and r.flags.c_contiguous and r.size >= self.nbytes
         return self._lib.drx_ldpc_decode(self.h, _ptrs(list(llr)), _ptrs(list(out)), n, int(max_iter))
 
-    def decode_host(self, llr, max_iter, stop=STOP_FRAME):
-        """Host batch: llr [n, nldpc] int8 -> (bits [n, nbytes], iters, ok)."""
+    def decode_host(self, llr, max_iter, stop=STOP_FRAME, out=None, iters=None, ok=None):
+        """Host batch: llr [n, nldpc] int8 -> (bits [n, nbytes], iters, ok).
+        out / iters / ok: optional preallocated C-contiguous arrays (uint8
+        [n, nbytes], int32 [n], uint8 [n]), reused by callers that decode
+        batch after batch."""
         llr = np.ascontiguousarray(llr, dtype=np.int8)
         n = llr.shape[0]
-        out = np.zeros((n, self.nbytes), np.uint8)
-        it = np.zeros(n, np.int32)
-        ok = np.zeros(n, np.uint8)
+        out = np.zeros((n, self.nbytes), np.uint8) if out is None else out
+        it = np.zeros(n, np.int32) if iters is None else iters
+        ok = np.zeros(n, np.uint8) if ok is None else ok
+        assert out.shape == (n, self.nbytes) and out.dtype == np.uint8 and out.flags.c_contiguous
+        assert it.shape == (n,) and it.dtype == np.int32 and ok.shape == (n,) and ok.dtype == np.uint8
         r = self._lib.drx_ldpc_decode_host(self.h, llr.ctypes.data, out.ctypes.data, it.ctypes.data,
                                            ok.ctypes.data, n, int(max_iter), int(stop))
         if r != 0:

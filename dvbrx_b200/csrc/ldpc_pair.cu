@@ -517,6 +517,8 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
          * last owned slot that can be late or early in this warp (most
          * layers share one pair of links: link slots 2 and 3 only) */
         const int lev = active ? (int)(meta & 0xFF) : -1;
+        uint32_t wa, wb; /* the check's learned words, read once for all its level steps */
+        lwords(wa, wb);
         auto steps = [&](auto ke) {
             constexpr int KE = decltype(ke)::value;
             for (int l = 0; l < nlev; l++) {
@@ -524,8 +526,6 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
                 if (__any_sync(0xFFFFFFFFu, mine)) {
                     if (l > 0)
                         ck.template read_late<KE>(fr.post, mine);
-                    uint32_t wa, wb;
-                    lwords(wa, wb);
                     ck.finish(0xFFFFFFFFu, mine, LEARNED, wa, wb);
                     ck.template write_early<KE>(fr.post, mine);
                 }

@@ -260,6 +260,29 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
         p.msg_stride = slab;
         return cuda_ok(launch_decode_pair(p, d->pair_kid, d->pair_smem, grid, s), "decoder launch") ? 0 : -1;
     }
+    const int pair_capacity = d->pair_ctas_per_sm * d->sms;
+    if (stop > 0 && use_pair(d) && (stop + 1) / 2 <= pair_capacity) {
+        /* groups of G frames on teams of ceil(G / 2) co-resident CTAs */
+        const int G = stop, M = (G + 1) / 2;
+        const int ngroups = (nframes + G - 1) / G;
+        const int nteams = std::min(ngroups, pair_capacity / M);
+        const int per_team = (ngroups + nteams - 1) / nteams;
+        const size_t words = 2 * (size_t)(max_iter + 1) * (size_t)nteams * per_team;
+        if (!ensure_sync(d, words))
+            return -1;
+        if (!cuda_ok(cudaMemsetAsync(d->sync, 0, words * sizeof(unsigned), s), "cudaMemsetAsync"))
+            return -1;
+        grid = nteams * M;
+        p.group = G;
+        p.nteams = nteams;
+        p.team_sync = d->sync;
+        const size_t slab = decode_pair_msg_bytes(d->code.R, d->pair_kid);
+        if (!ensure_scratch(d, slab * (size_t)grid))
+            return -1;
+        p.msg = d->msg;
+        p.msg_stride = slab;
+        return cuda_ok(launch_decode_pair(p, d->pair_kid, d->pair_smem, grid, s), "decoder launch") ? 0 : -1;
+    }
     if (stop == 0) {
         grid = std::min(nframes, capacity);
         p.group = 0;

@@ -605,6 +605,40 @@ __device__ void store_lane(const DevCode& c, const PairFrame& fr, int h, uint8_t
     }
 }
 
+/* Group barrier of a team of M co-resident CTAs (a cooperative launch):
+ * returns 1 if no member saw a failing frame, 0 if one did, -1 if the
+ * barrier gave up after kPairSpinLimit polls (the device error word is set). */
+constexpr int kPairSpinLimit = 1 << 22;
+__device__ int pair_team_vote(unsigned* slot, int M, bool fail, int* err)
+{
+    __shared__ int s_res;
+    if (threadIdx.x == 0) {
+        unsigned* arrive = slot;
+        unsigned* fails = slot + 1;
+        if (fail)
+            atomicAdd(fails, 1u);
+        __threadfence();
+        atomicAdd(arrive, 1u);
+        int spins = 0, res = 0;
+        while (*(volatile unsigned*)arrive < (unsigned)M) {
+            if (++spins > kPairSpinLimit) {
+                atomicExch(err, 2);
+                res = -1;
+                break;
+            }
+            __nanosleep(200);
+        }
+        __threadfence();
+        if (res == 0)
+            res = *(volatile unsigned*)fails == 0 ? 1 : 0;
+        s_res = res;
+    }
+    __syncthreads();
+    const int r = s_res;
+    __syncthreads();
+    return r;
+}
+
 template <int A, int B, int GDM, int LS, int T>
 __global__ void __launch_bounds__(T * 384, 1) k_decode_pair(DecodeParams p)
 {
@@ -622,6 +656,55 @@ __global__ void __launch_bounds__(T * 384, 1) k_decode_pair(DecodeParams p)
         s_reload = 3;
     }
     __syncthreads();
+    if (p.group > 0) {
+        /* group stopping (the reference's batch semantics): the G frames of a
+         * group run on a team of M = ceil(G / 2) CTAs, two frames each, and
+         * stop together at the first syndrome that every frame passes */
+        const int G = p.group, M = (G + 1) / 2;
+        const int team = blockIdx.x / M, member = blockIdx.x % M;
+        const int ngroups = (p.nframes + G - 1) / G;
+        const int per = p.max_iter + 1, per_team = (ngroups + p.nteams - 1) / p.nteams;
+        for (int g = team, k = 0; g < ngroups; g += p.nteams, k++) {
+            unsigned* sync = p.team_sync + 2 * (size_t)per * ((size_t)team * per_team + k);
+            const int end = min((g + 1) * G, p.nframes);
+            int fr2[2];
+            for (int h = 0; h < 2; h++) {
+                const int f = g * G + 2 * member + h;
+                fr2[h] = f < end ? f : -1;
+                const int row = fr2[h] < 0 ? 0 : p.rows ? p.rows[fr2[h]] : fr2[h];
+                load_lane(c, fr, fr2[h] >= 0 ? p.llr + (size_t)row * p.llr_stride : nullptr, h);
+            }
+            __syncthreads();
+            uint32_t gfresh = 0xFFFFFFFFu;
+            int it = 0;
+            bool ok = true;
+            for (;;) {
+                const int fail = syndrome_pair(c, fr, &s_flag);
+                if (t == 0)
+                    s_flag = 0; /* read again only after later barriers */
+                const int v = pair_team_vote(sync + 2 * it, M, fail != 0, p.err);
+                ok = v == 1;
+                if (v < 0 || ok || it >= p.max_iter)
+                    break;
+                iterate_pair<A, B, GDM, LS, T, false>(c, fr, msg, gfresh, -1, -1);
+                gfresh = 0;
+                it++;
+            }
+            for (int h = 0; h < 2; h++)
+                if (fr2[h] >= 0) {
+                    const int row = p.rows ? p.rows[fr2[h]] : fr2[h];
+                    store_lane(c, fr, h, p.out + (size_t)row * p.out_stride);
+                    if (t == 0) {
+                        if (p.iters)
+                            p.iters[row] = it;
+                        if (p.ok)
+                            p.ok[row] = ok ? 1 : 0;
+                    }
+                }
+            __syncthreads();
+        }
+        return;
+    }
     uint32_t fresh = 0;
     for (;;) {
         /* lanes that need a frame take the next one of the batch */
@@ -794,6 +877,8 @@ cudaError_t launch_decode_pair(const DecodeParams& p, int kid, size_t smem, int 
         return e;
     DecodeParams pc = p;
     void* args[] = { &pc };
+    if (p.group > 0)
+        return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kPairKernels[kid].threads), args, smem, stream);
     return cudaLaunchKernel(k, dim3(grid), dim3(kPairKernels[kid].threads), args, smem, stream);
 }
 

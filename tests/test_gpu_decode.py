@@ -139,6 +139,26 @@ def test_uniform_random_llrs(short, rate):
     assert (bits == rb).all() and (it == ri).all() and (ok == ro).all()
 
 
+@pytest.mark.parametrize("short,rate,es,n,G", [(1, "1_2", 1.6, 37, 5), (1, "1_2", 1.6, 37, 1), (0, "9_10", 6.6, 11, 3),
+                                             (0, "3_5", 5.8, 70, 64), (1, "8_9", 6.5, 20, 8)])
+def test_group_stopping_pair_matches_frame(short, rate, es, n, G):
+    """Group stopping on the frame-pair kernel (teams of ceil(G / 2) CTAs, an
+    odd G leaving the last lane empty, a partial last group) gives the
+    one-frame kernel's results, and the first group the reference's."""
+    llr = awgn_frames(short, rate, n, es, seed=zlib.crc32(rate.encode()) + 31 * G)
+    d = D.Ldpc(D.fec_lookup(short, rate), rate)
+    res = {}
+    for v in (D.VARIANT_FRAME, D.VARIANT_PAIR):
+        assert d.set_variant(v) == v
+        res[v] = d.decode_host(llr, 30, stop=G)
+    for a, b in zip(res[D.VARIANT_FRAME], res[D.VARIANT_PAIR]):
+        assert np.array_equal(a, b), (rate, G)
+    bits, it, ok = res[D.VARIANT_PAIR]
+    rb, rr = check_group(checker(short, rate), llr[:G], 30)
+    assert (int(it[0]) if ok[:G].all() else -1) == rr and (bits[:G] == rb).all()
+    d.close()
+
+
 def test_edge_cases():
     d = handle(1, "1_2")
     N = 16200

@@ -91,69 +91,106 @@ __device__ __forceinline__ int llr_pos(const DemapParams& p, int b, int j)
     return BITS == 2 ? 2 * j + b : p.order[b] * p.nsym + j;
 }
 
-/* Grid rows walk the frames (2/n0 once per block), threads take four
- * consecutive symbols: two 16-byte loads, and per label bit one 4-byte
- * store (eight bytes for QPSK) where the row layout allows it. */
+/* Grid rows walk the frames, threads take four consecutive symbols: two
+ * 16-byte loads, and per label bit one 4-byte store (eight bytes for QPSK)
+ * where the row layout allows it.  Every thread forms 2/n0 itself (one
+ * broadcast load), so the warps of a block never wait for one another and
+ * one warp's loads overlap another's arithmetic. */
+template <int BITS>
+__device__ __forceinline__ void demap_group(const DemapParams& p, const float4& a, const float4& c, int j0, float k,
+                                            int8_t* __restrict__ llr)
+{
+    int8_t v[4][BITS];
+    demap_symbol<BITS>(p, a.x, a.y, k, v[0]);
+    demap_symbol<BITS>(p, a.z, a.w, k, v[1]);
+    demap_symbol<BITS>(p, c.x, c.y, k, v[2]);
+    demap_symbol<BITS>(p, c.z, c.w, k, v[3]);
+    if (BITS == 2) {
+        uint2 w;
+        w.x = (uint32_t)(uint8_t)v[0][0] | (uint32_t)(uint8_t)v[0][1] << 8 | (uint32_t)(uint8_t)v[1][0] << 16 |
+              (uint32_t)(uint8_t)v[1][1] << 24;
+        w.y = (uint32_t)(uint8_t)v[2][0] | (uint32_t)(uint8_t)v[2][1] << 8 | (uint32_t)(uint8_t)v[3][0] << 16 |
+              (uint32_t)(uint8_t)v[3][1] << 24;
+        *(uint2*)(llr + 2 * (size_t)j0) = w;
+    } else {
+#pragma unroll
+        for (int b = 0; b < BITS; b++) {
+            const int pos = llr_pos<BITS>(p, b, j0);
+            if (pos + 3 < p.nldpc)
+                *(uint32_t*)(llr + pos) = (uint32_t)(uint8_t)v[0][b] | (uint32_t)(uint8_t)v[1][b] << 8 |
+                                          (uint32_t)(uint8_t)v[2][b] << 16 | (uint32_t)(uint8_t)v[3][b] << 24;
+            else
+                for (int s = 0; s < 4; s++)
+                    if (pos + s < p.nldpc)
+                        llr[pos + s] = v[s][b];
+        }
+    }
+}
+
+/* Grid rows walk the frames, thread g of a row takes symbols 4g .. 4g + 3
+ * of each of its frames (the launch covers every group of a frame): two
+ * 16-byte loads, and per label bit one 4-byte store (eight bytes for QPSK)
+ * where the row layout allows it.  The next frame's symbols are loaded
+ * before this frame's arithmetic, and every thread forms 2/n0 itself (one
+ * broadcast load), so loads stay in flight while the warps compute. */
 template <int BITS>
 __global__ void __launch_bounds__(256) k_demap(const __grid_constant__ DemapParams p)
 {
-    __shared__ float s_k;
     const int ngroups = (p.nsym + 3) / 4;
-    for (int f = blockIdx.y; f < p.nframes; f += gridDim.y) {
-        if (threadIdx.x == 0)
-            s_k = 2.0f / p.n0[f];
-        __syncthreads();
-        const float k = s_k;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups)
+        return;
+    const int j0 = 4 * g;
+    auto vec_of = [&](int f) {
         const float* sym = p.sym + (size_t)f * p.sym_stride;
+        const int8_t* llr = p.llr + (size_t)f * p.llr_stride;
+        return ((uintptr_t)sym & 15) == 0 && ((uintptr_t)llr & 7) == 0 && (p.nsym & 3) == 0;
+    };
+    int f = blockIdx.y;
+    if (f >= p.nframes)
+        return;
+    bool vec = vec_of(f);
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), c = a;
+    if (vec) {
+        const float* sym = p.sym + (size_t)f * p.sym_stride + 2 * (size_t)j0;
+        a = __ldcs((const float4*)sym);
+        c = __ldcs((const float4*)sym + 1);
+    }
+    for (; f < p.nframes; f += gridDim.y) {
+        const int fn = f + gridDim.y;
+        bool vecn = false;
+        float4 an = make_float4(0.f, 0.f, 0.f, 0.f), cn = an;
+        if (fn < p.nframes) {
+            vecn = vec_of(fn);
+            if (vecn) {
+                const float* sym = p.sym + (size_t)fn * p.sym_stride + 2 * (size_t)j0;
+                an = __ldcs((const float4*)sym);
+                cn = __ldcs((const float4*)sym + 1);
+            }
+        }
+        const float k = 2.0f / __ldg(p.n0 + f);
         int8_t* llr = p.llr + (size_t)f * p.llr_stride;
-        const bool vec = ((uintptr_t)sym & 15) == 0 && ((uintptr_t)llr & 7) == 0 && (p.nsym & 3) == 0;
-        for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
-            const int j0 = 4 * g;
-            int8_t v[4][BITS];
-            if (vec) {
-                const float4 a = *(const float4*)(sym + 2 * (size_t)j0);
-                const float4 c = *(const float4*)(sym + 2 * (size_t)j0 + 4);
-                demap_symbol<BITS>(p, a.x, a.y, k, v[0]);
-                demap_symbol<BITS>(p, a.z, a.w, k, v[1]);
-                demap_symbol<BITS>(p, c.x, c.y, k, v[2]);
-                demap_symbol<BITS>(p, c.z, c.w, k, v[3]);
-                if (BITS == 2) {
-                    uint2 w;
-                    w.x = (uint32_t)(uint8_t)v[0][0] | (uint32_t)(uint8_t)v[0][1] << 8 |
-                          (uint32_t)(uint8_t)v[1][0] << 16 | (uint32_t)(uint8_t)v[1][1] << 24;
-                    w.y = (uint32_t)(uint8_t)v[2][0] | (uint32_t)(uint8_t)v[2][1] << 8 |
-                          (uint32_t)(uint8_t)v[3][0] << 16 | (uint32_t)(uint8_t)v[3][1] << 24;
-                    *(uint2*)(llr + 2 * (size_t)j0) = w;
-                } else {
+        if (vec) {
+            demap_group<BITS>(p, a, c, j0, k, llr);
+        } else {
+            const float* sym = p.sym + (size_t)f * p.sym_stride;
+            int8_t v[BITS];
+            for (int s = 0; s < 4; s++) {
+                const int j = j0 + s;
+                if (j >= p.nsym)
+                    break;
+                demap_symbol<BITS>(p, sym[2 * (size_t)j], sym[2 * (size_t)j + 1], k, v);
 #pragma unroll
-                    for (int b = 0; b < BITS; b++) {
-                        const int pos = llr_pos<BITS>(p, b, j0);
-                        if (pos + 3 < p.nldpc)
-                            *(uint32_t*)(llr + pos) = (uint32_t)(uint8_t)v[0][b] | (uint32_t)(uint8_t)v[1][b] << 8 |
-                                                      (uint32_t)(uint8_t)v[2][b] << 16 |
-                                                      (uint32_t)(uint8_t)v[3][b] << 24;
-                        else
-                            for (int s = 0; s < 4; s++)
-                                if (pos + s < p.nldpc)
-                                    llr[pos + s] = v[s][b];
-                    }
-                }
-            } else {
-                for (int s = 0; s < 4; s++) {
-                    const int j = j0 + s;
-                    if (j >= p.nsym)
-                        break;
-                    demap_symbol<BITS>(p, sym[2 * (size_t)j], sym[2 * (size_t)j + 1], k, v[s]);
-#pragma unroll
-                    for (int b = 0; b < BITS; b++) {
-                        const int pos = llr_pos<BITS>(p, b, j);
-                        if (pos < p.nldpc)
-                            llr[pos] = v[s][b];
-                    }
+                for (int b = 0; b < BITS; b++) {
+                    const int pos = llr_pos<BITS>(p, b, j);
+                    if (pos < p.nldpc)
+                        llr[pos] = v[b];
                 }
             }
         }
-        __syncthreads(); /* s_k is rewritten for the next frame */
+        a = an;
+        c = cn;
+        vec = vecn;
     }
 }
 

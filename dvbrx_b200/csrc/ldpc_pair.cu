@@ -14,12 +14,11 @@
  * v holds the int8 posterior of variable v for lane A (low byte) and lane B
  * (high byte): K information bits, then R parity bits in layer order.
  *
- * A check node runs on one thread (T = 1): 360 of the 384 threads hold the
- * 360 checks of a layer, every link of a check in registers, no shuffles.
- * (The template also builds T = 2, a check's links alternating over two
- * threads that combine their minimums with one shuffle round; on 3/5 and
- * 18/30 it runs 17-22 % slower: twice the per-check set-up and finish work
- * for the same link work.)  Levelled layers run in phases (layer_pair): the
+ * A check node runs on one thread: 360 of the 384 threads hold the 360
+ * checks of a layer, every link of a check in registers, no shuffles (two
+ * threads per check, combining their minimums with a shuffle round, ran
+ * 17-22 % slower on 3/5 and 18/30: twice the per-check set-up and finish
+ * work for the same link work).  Levelled layers run in phases (layer_pair): the
  * wavefront levels carry only the links two checks of the layer share.  The
  * thread of a check stores its compressed messages for both frames in one
  * 8-byte record: per lane min0 (6 bits) | min1 << 6 | index << 12, then the
@@ -92,20 +91,16 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
 }
 
 /*
- * One check node (i, j) for both lanes, on T threads (r = 0 .. T-1): thread
- * r owns the node's link slots c = r + T k, k = 0 .. S-1.  Slot 0 is the
- * parity bit, slot 1 the previous parity bit (absent for (0, 0)), 2 + e
- * information entry e of the layer.  DM is the node degree (EXACT) or a
- * bound on it (the degree is then a run-time value).  The node state lives
- * in registers across the phases of its layer (see layer_pair).
- *
- * Slot masks keep owned slot k at bit T k (the layer's 24-bit slot masks
- * shifted right by r); the message's sign bits and index are shifted by r
- * the same way, so everything a slot needs besides its address depends on
- * k alone.  The full passes run every slot without branches: a slot that is
- * not a link, or whose bit an earlier check of the layer writes (read later,
- * in its level), enters the minimums as 255, which no magnitude reaches;
- * stores are predicated.
+ * One check node (i, j) for both lanes, on one thread: link slots
+ * k = 0 .. S-1.  Slot 0 is the parity bit, slot 1 the previous parity bit
+ * (absent for (0, 0)), 2 + e information entry e of the layer.  DM is the
+ * node degree (EXACT) or a bound on it (the degree is then a run-time
+ * value).  The node state lives in registers across the phases of its layer
+ * (see layer_pair).  Slot masks, sign bits and the message index keep slot
+ * k at bit k.  The full passes run every slot without branches: a slot that
+ * is not a link, or whose bit an earlier check of the layer writes (read
+ * later, in its level), enters the minimums as 255, which no magnitude
+ * reaches; stores are predicated.
  */
 /* A check's message record: 8 bytes up to degree 16 (per lane min0, min1
  * and a 4-bit index in one word, 16 sign bits per lane in the other); 16
@@ -115,60 +110,53 @@ template <bool WIDE>
 using PairRec = typename std::conditional<WIDE, uint4, uint2>::type;
 
 /* WIDE: the kernel's records are 16 bytes (its degree bound is above 16) */
-template <int DM, bool EXACT, int LS, int T, bool WIDE>
+template <int DM, bool EXACT, int LS, bool WIDE>
 struct PairCheck {
-    static_assert(!WIDE || T == 1, "records of more than 16 links are built by one thread");
     static_assert(DM <= (WIDE ? 32 : 16), "degree above the record's slots");
     using Rec = PairRec<WIDE>;
-    static constexpr int S = T == 2 ? (DM + 1) / 2 : DM;
-    /* owned slots that can be late or early: k0 .. k1 (link slots 2 .. 2 LS + 1) */
-    static constexpr int K0 = T == 2 ? 1 : 2;
-    static constexpr int K1 = T == 2 ? (S - 1 < LS ? S - 1 : LS) : (S - 1 < 2 * LS + 1 ? S - 1 : 2 * LS + 1);
-    int r;
+    static constexpr int S = DM;
+    /* slots that can be late or early: K0 .. K1 (link slots 2 .. 2 LS + 1) */
+    static constexpr int K0 = 2;
+    static constexpr int K1 = S - 1 < 2 * LS + 1 ? S - 1 : 2 * LS + 1;
     uint32_t addr[S]; /* shared-memory byte addresses of the owned links' posteriors */
     uint32_t x[S];
-    uint32_t live, inm, outm; /* bit 2k: owned slot k is a link / is read late / is written early */
+    uint32_t live, inm, outm; /* bit k: slot k is a link / is read late / is written early */
     uint32_t n0, n1, p0, p1, idxh, sgn, sgn1; /* sgn: sign bits of slots 0-15, sgn1: 16-31 */
     uint32_t min0, min1, sg, mn0, mn1;
     uint32_t m0p1, nmn0, nmn1; /* min0 + 1, -mn0, -mn1 (set by finish) */
 
     __device__ __forceinline__ void setup(const int2* __restrict__ ent, int cnt, int K, int q, int i, int j,
-                                          int rr, Rec rec, uint32_t fresh, unsigned long long meta,
-                                          uint32_t sbase)
+                                          Rec rec, uint32_t fresh, unsigned long long meta, uint32_t sbase)
     {
-        r = rr;
         const int D = EXACT ? DM : cnt + 2;
         const int pc = K + kQCp * i + j;
         const int pp = i ? pc - kQCp : K + kQCp * (q - 1) + j - 1;
         uint32_t lv = (1u << D) - 1u;
         if ((i | j) == 0)
             lv &= ~2u;
-        live = lv >> r;
-        inm = ((uint32_t)(meta >> 8) & 0xFFFFFFu) >> r;
-        outm = ((uint32_t)(meta >> 32) & 0xFFFFFFu) >> r;
+        live = lv;
+        inm = (uint32_t)(meta >> 8) & 0xFFFFFFu;
+        outm = (uint32_t)(meta >> 32) & 0xFFFFFFu;
 #pragma unroll
         for (int k = 0; k < S; k++) {
-            const int c = r + T * k;
-            if (T == 2 && k == 0) {
-                addr[k] = sbase + 2u * (uint32_t)(r == 0 ? pc : pp);
-            } else if (T == 1 && k < 2) {
+            if (k < 2) {
                 addr[k] = sbase + 2u * (uint32_t)(k == 0 ? pc : pp);
             } else {
                 /* a slot past the degree takes the last link's address: read, never used */
-                const int2 e = ent[min(c, D - 1) - 2];
+                const int2 e = ent[min(k, D - 1) - 2];
                 addr[k] = (uint32_t)e.x + 2u * (uint32_t)j + (j < e.y ? 2u * kQCp : 0u);
             }
         }
         /* messages: zero for a lane in its first iteration */
         const uint32_t w0 = rec.x & ~fresh;
-        sgn = (rec.y & ~fresh) >> r;
+        sgn = rec.y & ~fresh;
         const uint32_t m0 = w0 & 0x003F003Fu, m1 = (w0 >> 6) & 0x003F003Fu;
         if constexpr (WIDE) {
             sgn1 = rec.z & ~fresh;
             idxh = (rec.w & ~fresh) | 0x64006400u; /* FP16 1024 + index */
         } else {
             sgn1 = 0;
-            idxh = (((w0 >> 12) & 0x000F000Fu) | 0x64006400u) - (uint32_t)r * 0x00010001u; /* FP16 1024 + index - r */
+            idxh = ((w0 >> 12) & 0x000F000Fu) | 0x64006400u; /* FP16 1024 + index */
         }
         /* minus the message: +m if it is negative, else -min(m, 31) */
         n0 = m0;
@@ -179,11 +167,11 @@ struct PairCheck {
         sg = 0;
     }
 
-    /* minus the old message of owned slot k */
+    /* minus the old message of slot k */
     __device__ __forceinline__ uint32_t unmsg(int k) const
     {
-        const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)(T * k) * 0x00010001u);
-        const uint32_t sm = lmask((T * k < 16 ? sgn : sgn1) << (15 - ((T * k) & 15)));
+        const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)k * 0x00010001u);
+        const uint32_t sm = lmask((k < 16 ? sgn : sgn1) << (15 - (k & 15)));
         return sel(sm, sel(im, n1, n0), sel(im, p1, p0));
     }
 
@@ -195,11 +183,11 @@ struct PairCheck {
         sg ^= v;
     }
 
-    /* every owned slot but the late ones, without branches; minimums folded
+    /* every slot but the late ones, without branches; minimums folded
      * two slots at a time: min1 = second smallest of {min0, min1, a, b} =
      * min3(max(min0, min(a, b)), min1, max(a, b)).  LEV: the layer has late
      * slots; otherwise only the slots that can be absent are masked (the
-     * previous parity of check (0, 0), the odd slot past the degree). */
+     * previous parity of check (0, 0)). */
     template <bool LEV>
     __device__ __forceinline__ void read_all(const uint16_t* __restrict__ post)
     {
@@ -209,11 +197,11 @@ struct PairCheck {
         for (int k = 0; k < S; k++) {
             const uint32_t m = unmsg(k);
             uint32_t v = sadd(sx2(lds16(addr[k])), m);
-            if (LEV || !EXACT || (T == 2 ? k == 0 || (k == S - 1 && (DM & 1)) : k == 1))
-                v = ((excl >> (T * k)) & 1u) ? 0x00FF00FFu : v;
+            if (LEV || !EXACT || k == 1)
+                v = ((excl >> k) & 1u) ? 0x00FF00FFu : v;
             f[k] = v;
             /* a late slot keeps minus its old message for read_late */
-            x[k] = LEV && ((inm >> (T * k)) & 1u) ? m : v;
+            x[k] = LEV && ((inm >> k) & 1u) ? m : v;
         }
 #pragma unroll
         for (int k = 0; k + 1 < S; k += 2) {
@@ -227,11 +215,10 @@ struct PairCheck {
             fold(f[S - 1]);
     }
 
-    /* a thread that holds no check (t >= 360 T): valid addresses, no links,
-     * so that it can run the warp-uniform level steps of its warp */
+    /* a thread that holds no check (t >= 360): valid addresses, no links, so
+     * that it can run the warp-uniform level steps of its warp */
     __device__ __forceinline__ void idle(uint32_t sbase)
     {
-        r = 0;
 #pragma unroll
         for (int k = 0; k < S; k++) {
             addr[k] = sbase;
@@ -247,32 +234,26 @@ struct PairCheck {
     /* the late slots (their bits were written by earlier levels) of a check
      * in the current level (mine); other threads keep their state.  Shared
      * links come first in every layer (codes.cpp), so late and early slots
-     * are among slots 2 .. 2 KL + 1 (owned slots 1 .. KL) */
+     * are among slots 2 .. KE */
     template <int KE>
     __device__ __forceinline__ void read_late(const uint16_t* __restrict__ post, bool mine)
     {
         const uint32_t im = mine ? inm : 0u;
 #pragma unroll
         for (int k = K0; k <= KE; k++) {
-            const bool in = (im >> (T * k)) & 1u;
+            const bool in = (im >> k) & 1u;
             const uint32_t v = sadd(sx2(lds16(addr[k])), x[k]);
             x[k] = in ? v : x[k];
             fold(in ? v : 0x00FF00FFu);
         }
     }
 
-    /* combine with the partner thread (T = 2); the cap at 127 and offset 1, or the
-     * learned scale and offset of each lane's iteration (lpA, lpB).  Only
-     * threads with `take` keep the result: the level steps run it on whole
-     * warps (full-mask shuffles; a shuffle under a partial mask inside a
-     * divergent branch costs several times as much) */
-    __device__ __forceinline__ void finish(unsigned gmask, bool take, bool learned, uint32_t lpA, uint32_t lpB)
+    /* the cap at 127 and offset 1, or the learned scale and offset of each
+     * lane's iteration (lpA, lpB).  Only threads with `take` keep the result:
+     * the level steps run it on whole warps */
+    __device__ __forceinline__ void finish(bool take, bool learned, uint32_t lpA, uint32_t lpB)
     {
-        const uint32_t b0 = T == 2 ? __shfl_xor_sync(gmask, min0, 1) : 0x00FF00FFu;
-        const uint32_t b1 = T == 2 ? __shfl_xor_sync(gmask, min1, 1) : 0x00FF00FFu;
-        const uint32_t bs = T == 2 ? __shfl_xor_sync(gmask, sg, 1) : 0u;
-        const uint32_t c1 = __vmins2(__vmaxs2(min0, b0), __vmins2(min1, b1));
-        const uint32_t c0 = __vmins2(min0, b0);
+        const uint32_t c1 = min1, c0 = min0;
         uint32_t m0, m1;
         if (learned) {
             const uint32_t k0 = __vmins2(c0, 0x007F007Fu), k1 = __vmins2(c1, 0x007F007Fu);
@@ -283,9 +264,6 @@ struct PairCheck {
             m1 = __viaddmax_s16x2(__vmins2(c1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
         }
         if (take) {
-            min0 = c0;
-            min1 = c1;
-            sg ^= bs;
             mn0 = m0;
             mn1 = m1;
             m0p1 = __vadd2(c0, 0x00010001u);
@@ -294,7 +272,7 @@ struct PairCheck {
         }
     }
 
-    /* new posterior of owned slot k (two bytes), and its masks: lanes where
+    /* new posterior of slot k (two bytes), and its masks: lanes where
      * |x| is above min0 (the slot does not hold the minimum) and lanes whose
      * outgoing message is negative */
     __device__ __forceinline__ uint32_t update(int k, uint32_t& above, uint32_t& neg) const
@@ -317,7 +295,7 @@ struct PairCheck {
         for (int k = K0; k <= KE; k++) {
             uint32_t above, neg;
             const uint32_t nv = update(k, above, neg);
-            if ((om >> (T * k)) & 1u)
+            if ((om >> k) & 1u)
                 sts16(addr[k], nv);
         }
     }
@@ -325,37 +303,28 @@ struct PairCheck {
     /* every other posterior (predicated stores) and the node's compressed
      * messages for both lanes, stored by thread 0: the slot holding min0 and
      * one sign bit per slot */
-    __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, unsigned gmask, Rec* __restrict__ dst)
+    __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, Rec* __restrict__ dst)
     {
         const uint32_t wm = live & ~outm;
-        uint32_t nidx = 0, nsg = 0, nsg1 = 0; /* nidx per lane: T k + 1 of an owned slot holding min0, 0 if none */
+        uint32_t nidx = 0, nsg = 0, nsg1 = 0; /* nidx per lane: k + 1 of a slot holding min0, 0 if none */
 #pragma unroll
         for (int k = 0; k < S; k++) {
             uint32_t above, neg;
             const uint32_t nv = update(k, above, neg);
-            if ((wm >> (T * k)) & 1u)
+            if ((wm >> k) & 1u)
                 sts16(addr[k], nv);
-            nidx = sel(above, nidx, (uint32_t)(T * k + 1) * 0x00010001u);
-            if (T * k < 16)
-                nsg |= neg & (0x00010001u << (T * k));
+            nidx = sel(above, nidx, (uint32_t)(k + 1) * 0x00010001u);
+            if (k < 16)
+                nsg |= neg & (0x00010001u << k);
             else
-                nsg1 |= neg & (0x00010001u << (T * k - 16));
-        }
-        if (T == 2) {
-            nsg <<= r; /* bit 2k -> slot 2k + r (slots stay below 16: no carry across lanes) */
-            const uint32_t found = lmask(__vsub2(0u, nidx)); /* lanes with nidx > 0 */
-            nidx = __vadd2(nidx, found & ((uint32_t)r * 0x00010001u)); /* 2k + r + 1 */
-            nidx = __vmaxs2(nidx, __shfl_xor_sync(gmask, nidx, 1));
-            nsg |= __shfl_xor_sync(gmask, nsg, 1);
+                nsg1 |= neg & (0x00010001u << (k - 16));
         }
         nidx = __viaddmax_s16x2(nidx, 0xFFFFFFFFu, 0u); /* slot number: max(nidx - 1, 0) */
-        if (r == 0) {
-            const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
-            if constexpr (WIDE)
-                __stcg(dst, make_uint4(m0c | (m1c << 6), nsg, nsg1, nidx));
-            else
-                __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
-        }
+        const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
+        if constexpr (WIDE)
+            __stcg(dst, make_uint4(m0c | (m1c << 6), nsg, nsg1, nidx));
+        else
+            __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
     }
 };
 
@@ -482,15 +451,15 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
  * constrain the bits two checks of a layer share, so the wavefront levels
  * carry just those links.  Unlevelled layers take one pass.
  */
-template <int DM, bool EXACT, int LS, int T, bool WIDE, bool LEARNED>
+template <int DM, bool EXACT, int LS, bool WIDE, bool LEARNED>
 __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev,
                                            PairRec<WIDE> rec, unsigned long long meta, uint32_t fresh,
                                            PairRec<WIDE>* __restrict__ msg,
                                            int lA, int lB)
 {
     const int t = threadIdx.x;
-    const bool active = t < T * kQCp;
-    const int j = T == 2 ? t >> 1 : t;
+    const bool active = t < kQCp;
+    const int j = t;
     /* learned scale / offset words of the check for both lanes */
     auto lwords = [&](uint32_t& a, uint32_t& b) {
         a = b = 0;
@@ -500,9 +469,10 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             b = s_learn_tab[lB + k];
         }
     };
-    PairCheck<DM, EXACT, LS, T, WIDE> ck;
+    using Ck = PairCheck<DM, EXACT, LS, WIDE>;
+    Ck ck;
     if (active) {
-        ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, T == 2 ? t & 1 : 0, rec, fresh, meta,
+        ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, rec, fresh, meta,
                  (uint32_t)__cvta_generic_to_shared(fr.post));
         if (nlev > 1)
             ck.template read_all<true>(fr.post);
@@ -514,7 +484,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
     if (nlev > 1) {
         /* a level step runs on every warp that holds a check of the level,
          * with all its lanes; the other checks keep their state.  KE: the
-         * last owned slot that can be late or early in this warp (most
+         * last slot that can be late or early in this warp (most
          * layers share one pair of links: link slots 2 and 3 only) */
         const int lev = active ? (int)(meta & 0xFF) : -1;
         uint32_t wa, wb; /* the check's learned words, read once for all its level steps */
@@ -526,30 +496,25 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
                 if (__any_sync(0xFFFFFFFFu, mine)) {
                     if (l > 0)
                         ck.template read_late<KE>(fr.post, mine);
-                    ck.finish(0xFFFFFFFFu, mine, LEARNED, wa, wb);
+                    ck.finish(mine, LEARNED, wa, wb);
                     ck.template write_early<KE>(fr.post, mine);
                 }
                 __syncthreads();
             }
         };
-        using Ck = PairCheck<DM, EXACT, LS, T, WIDE>;
-        constexpr int KS = T == 1 && Ck::K1 > 3 ? 3 : Ck::K1;
+        constexpr int KS = Ck::K1 > 3 ? 3 : Ck::K1;
         const uint32_t lm = __reduce_or_sync(0xFFFFFFFFu, ck.inm | ck.outm);
-        if (KS < Ck::K1 && (lm >> (T * (KS + 1))) != 0)
+        if (KS < Ck::K1 && (lm >> (KS + 1)) != 0)
             steps(std::integral_constant<int, Ck::K1>());
         else
             steps(std::integral_constant<int, KS>());
-    } else {
-        const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
-        if (active) {
-            uint32_t wa, wb;
-            lwords(wa, wb);
-            ck.finish(gm, true, LEARNED, wa, wb);
-        }
+    } else if (active) {
+        uint32_t wa, wb;
+        lwords(wa, wb);
+        ck.finish(true, LEARNED, wa, wb);
     }
-    const unsigned gm = __ballot_sync(0xFFFFFFFFu, active);
     if (active)
-        ck.write_rest(fr.post, gm, msg + kQCp * i + j);
+        ck.write_rest(fr.post, msg + kQCp * i + j);
     __syncthreads();
 }
 
@@ -557,15 +522,15 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
  * level metadata are fetched one layer ahead.  The kernel is compiled for
  * the two information-link counts A <= B of its codes (exact-degree check
  * nodes), or, with GDM > 0, for any count up to GDM - 2 (predicated). */
-template <int A, int B, int GDM, int LS, int T, bool LEARNED>
+template <int A, int B, int GDM, int LS, bool LEARNED>
 __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, uint32_t fresh, int lA, int lB)
 {
     constexpr bool WIDE = (GDM > 0 ? GDM : B + 2) > 16;
     using Rec = PairRec<WIDE>;
     Rec* __restrict__ msg = (Rec*)msgv;
     const int t = threadIdx.x;
-    const int j = T == 2 ? t >> 1 : t;
-    const bool active = t < T * kQCp;
+    const int j = t;
+    const bool active = t < kQCp;
     Rec rn{};
     unsigned long long mn = 0;
     if (active) {
@@ -582,11 +547,11 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, 
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
         const int nlev = c.nlev[i];
         if (GDM > 0)
-            layer_pair<(GDM > 0 ? GDM : 2), false, LS, T, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<(GDM > 0 ? GDM : 2), false, LS, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else if (A == B || cnt == A)
-            layer_pair<A + 2, true, LS, T, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<A + 2, true, LS, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
         else
-            layer_pair<B + 2, true, LS, T, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<B + 2, true, LS, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
     }
 }
 
@@ -639,8 +604,8 @@ __device__ int pair_team_vote(unsigned* slot, int M, bool fail, int* err)
     return r;
 }
 
-template <int A, int B, int GDM, int LS, int T>
-__global__ void __launch_bounds__(T * 384, 1) k_decode_pair(DecodeParams p)
+template <int A, int B, int GDM, int LS>
+__global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
 {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_frame[2], s_iter[2], s_flag, s_reload;
@@ -686,7 +651,7 @@ __global__ void __launch_bounds__(T * 384, 1) k_decode_pair(DecodeParams p)
                 ok = v == 1;
                 if (v < 0 || ok || it >= p.max_iter)
                     break;
-                iterate_pair<A, B, GDM, LS, T, false>(c, fr, msg, gfresh, -1, -1);
+                iterate_pair<A, B, GDM, LS, false>(c, fr, msg, gfresh, -1, -1);
                 gfresh = 0;
                 it++;
             }
@@ -758,9 +723,9 @@ __global__ void __launch_bounds__(T * 384, 1) k_decode_pair(DecodeParams p)
         if (done)
             continue; /* reload, then check the new frames first */
         if (lT)
-            iterate_pair<A, B, GDM, LS, T, true>(c, fr, msg, fresh, learn_row(s_iter[0], lT), learn_row(s_iter[1], lT));
+            iterate_pair<A, B, GDM, LS, true>(c, fr, msg, fresh, learn_row(s_iter[0], lT), learn_row(s_iter[1], lT));
         else
-            iterate_pair<A, B, GDM, LS, T, false>(c, fr, msg, fresh, -1, -1);
+            iterate_pair<A, B, GDM, LS, false>(c, fr, msg, fresh, -1, -1);
         fresh = 0;
         if (t == 0) {
             s_iter[0]++;
@@ -788,10 +753,10 @@ struct PairKernel {
     const void* fn;
 };
 
-#define DRXG_PKL(a, b, ls) { a, b, 0, ls, 384, (const void*)k_decode_pair<a, b, 0, ls, 1> }
+#define DRXG_PKL(a, b, ls) { a, b, 0, ls, 384, (const void*)k_decode_pair<a, b, 0, ls> }
 #define DRXG_PK(a, b) DRXG_PKL(a, b, 2)
 #define DRXG_PK3(a, b) DRXG_PKL(a, b, 3)
-#define DRXG_PGL(d, ls) { 0, 0, d, ls, 384, (const void*)k_decode_pair<1, 1, d, ls, 1> }
+#define DRXG_PGL(d, ls) { 0, 0, d, ls, 384, (const void*)k_decode_pair<1, 1, d, ls> }
 #define DRXG_PG(d) DRXG_PGL(d, 3)
 static const PairKernel kPairKernels[] = {
     DRXG_PK(1, 2), DRXG_PK(2, 2), DRXG_PK(2, 3), DRXG_PK(3, 3), DRXG_PK(4, 4), DRXG_PK(5, 5),

@@ -628,11 +628,13 @@ def run_b200(args):
     # end to end through the C ABI with host buffers (synchronous call)
     e2e = None
     if args.e2e_steps > 0:
-        host = [l.cpu().numpy() for l in llr]
-        # output buffers allocated once and reused, as a receiver decoding batch after batch does
-        h_out = np.zeros((F, dec.nbytes), np.uint8)
-        h_it = np.zeros(F, np.int32)
-        h_ok = np.zeros(F, np.uint8)
+        # pinned host rows in and out (the copy engines read and write them directly), the output
+        # buffers allocated once and reused, as a receiver decoding batch after batch does
+        host_t = [l.cpu().pin_memory() for l in llr]
+        host = [t.numpy() for t in host_t]
+        out_t = [torch.zeros((F, dec.nbytes), dtype=torch.uint8).pin_memory(),
+                 torch.zeros(F, dtype=torch.int32).pin_memory(), torch.zeros(F, dtype=torch.uint8).pin_memory()]
+        h_out, h_it, h_ok = (t.numpy() for t in out_t)
         for k in range(min(2, args.e2e_steps)):
             dec.decode_host(host[k % len(host)], MAX_ITER, out=h_out, iters=h_it, ok=h_ok)
         if world > 1:
@@ -644,7 +646,8 @@ def run_b200(args):
         e2e = {"value": aggregate_gbps(world, args.e2e_steps * F, kldpc, dt * 1e3), "unit": UNIT,
                "h2d_bytes_per_step": F * dec.N,
                "d2h_bytes_per_step": F * (dec.nbytes + 4 + 1),
-               "api": "drx_ldpc_decode_host (host rows in, host bits/iterations/flags out; wall clock)"}
+               "api": "drx_ldpc_decode_host (pinned host rows in, pinned host bits/iterations/flags out; "
+                      "wall clock)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -397,14 +397,30 @@ void par_memcpy(void* dst, const void* src, size_t n)
         t.join();
 }
 
+/* True if p is page-locked host memory (cudaMallocHost, cudaHostAlloc,
+ * cudaHostRegister), which the copy engines read and write directly. */
+bool host_pinned(const void* p)
+{
+    if (!p)
+        return true;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError(); /* not a pointer the runtime knows: pageable */
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
 /*
  * Host batch, pipelined: the batch goes in chunks, each staged into pinned
- * memory on the host, copied in on the copy stream and decoded on one of two
- * alternating streams (each with its own message slab), so that copies
- * overlap decodes and a chunk's tail overlaps the next chunk.  The first
- * chunk is one wave of the decoder (every CTA busy once), so that the GPU
- * starts early; chunks then double.  Each chunk's results are copied back
- * on its decode stream and out of pinned memory while later chunks decode.
+ * memory on the host (unless the caller's rows are pinned already: then the
+ * copy engine reads them directly), copied in on the copy stream and decoded
+ * on one of two alternating streams (each with its own message slab), so
+ * that copies overlap decodes and a chunk's tail overlaps the next chunk.
+ * The first chunk is one wave of the decoder (every CTA busy once), so that
+ * the GPU starts early; chunks then double.  Each chunk's results are copied
+ * back on its decode stream (into the caller's arrays if they are pinned)
+ * and out of the staging memory while later chunks decode.
  */
 int decode_host_pipelined(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t* iters, uint8_t* ok, int nframes,
                           int max_iter)
@@ -440,34 +456,43 @@ int decode_host_pipelined(drx_ldpc* d, const int8_t* llr, uint8_t* out, int32_t*
         !cuda_ok(cudaStreamWaitEvent(d->pipe[0], start, 0), "cudaStreamWaitEvent") ||
         !cuda_ok(cudaStreamWaitEvent(d->pipe[1], start, 0), "cudaStreamWaitEvent"))
         return -1;
+    const bool in_pinned = host_pinned(llr);
+    const bool out_pinned = host_pinned(out) && host_pinned(iters) && host_pinned(ok);
+    const int8_t* h_in = in_pinned ? llr : d->h_llr;
+    uint8_t* h_out = out_pinned ? out : d->h_out;
+    int32_t* h_it = out_pinned ? iters : d->h_it;
+    uint8_t* h_ok = out_pinned ? ok : d->h_ok;
     int rc = 0, queued = 0;
     for (int c = 0; c < nch && rc == 0; c++, queued++) {
         const size_t a = (size_t)first[c];
         const int n = size[c];
-        par_memcpy(d->h_llr + a * N, llr + a * N, (size_t)n * N);
+        if (!in_pinned)
+            par_memcpy(d->h_llr + a * N, llr + a * N, (size_t)n * N);
         cudaStream_t ks = d->pipe[c & 1];
         Extra x;
         x.work = d->chunk_work + c;
         x.msg = (c & 1) ? d->msg2 : d->msg;
-        if (!cuda_ok(cudaMemcpyAsync(d->d_llr + a * N, d->h_llr + a * N, (size_t)n * N, cudaMemcpyHostToDevice,
-                                     d->copy),
-                     "cudaMemcpyAsync") ||
-            !cuda_ok(cudaEventRecord(in_ev[c], d->copy), "cudaEventRecord") ||
-            !cuda_ok(cudaStreamWaitEvent(ks, in_ev[c], 0), "cudaStreamWaitEvent") ||
-            enqueue(d, d->d_llr + a * N, N, d->d_out + a * nb, nb, d->d_it + a, d->d_ok + a, n, max_iter, 0, ks,
-                    &x) ||
-            !cuda_ok(cudaMemcpyAsync(d->h_out + a * nb, d->d_out + a * nb, (size_t)n * nb, cudaMemcpyDeviceToHost,
-                                     ks),
-                     "cudaMemcpyAsync") ||
-            !cuda_ok(cudaMemcpyAsync(d->h_it + a, d->d_it + a, (size_t)n * 4, cudaMemcpyDeviceToHost, ks),
-                     "cudaMemcpyAsync") ||
-            !cuda_ok(cudaMemcpyAsync(d->h_ok + a, d->d_ok + a, (size_t)n, cudaMemcpyDeviceToHost, ks),
-                     "cudaMemcpyAsync") ||
-            !cuda_ok(cudaEventRecord(out_ev[c], ks), "cudaEventRecord"))
+        bool good = cuda_ok(cudaMemcpyAsync(d->d_llr + a * N, h_in + a * N, (size_t)n * N, cudaMemcpyHostToDevice,
+                                            d->copy),
+                            "cudaMemcpyAsync") &&
+                    cuda_ok(cudaEventRecord(in_ev[c], d->copy), "cudaEventRecord") &&
+                    cuda_ok(cudaStreamWaitEvent(ks, in_ev[c], 0), "cudaStreamWaitEvent") &&
+                    !enqueue(d, d->d_llr + a * N, N, d->d_out + a * nb, nb, d->d_it + a, d->d_ok + a, n, max_iter,
+                             0, ks, &x) &&
+                    cuda_ok(cudaMemcpyAsync(h_out + a * nb, d->d_out + a * nb, (size_t)n * nb,
+                                            cudaMemcpyDeviceToHost, ks),
+                            "cudaMemcpyAsync");
+        if (good && h_it)
+            good = cuda_ok(cudaMemcpyAsync(h_it + a, d->d_it + a, (size_t)n * 4, cudaMemcpyDeviceToHost, ks),
+                           "cudaMemcpyAsync");
+        if (good && h_ok)
+            good = cuda_ok(cudaMemcpyAsync(h_ok + a, d->d_ok + a, (size_t)n, cudaMemcpyDeviceToHost, ks),
+                           "cudaMemcpyAsync");
+        if (!good || !cuda_ok(cudaEventRecord(out_ev[c], ks), "cudaEventRecord"))
             rc = -1;
     }
-    /* results out of pinned memory, chunk by chunk, as they arrive */
-    for (int c = 0; c < queued && rc == 0; c++) {
+    /* results out of the staging memory, chunk by chunk, as they arrive */
+    for (int c = 0; c < queued && rc == 0 && !out_pinned; c++) {
         if (!cuda_ok(cudaEventSynchronize(out_ev[c]), "decode")) {
             rc = -1;
             break;

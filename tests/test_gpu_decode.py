@@ -250,6 +250,14 @@ def test_host_call_pipelined_matches_device(short, rate, n):
     assert np.array_equal(bits, tb.cpu().numpy())
     assert np.array_equal(it, ti.cpu().numpy())
     assert np.array_equal(ok, to.cpu().numpy())
+    # page-locked rows in and out: the copy engines read and write the caller's arrays directly
+    pin = [torch.from_numpy(llr).pin_memory(), torch.zeros((n, d.nbytes), dtype=torch.uint8).pin_memory(),
+           torch.zeros(n, dtype=torch.int32).pin_memory(), torch.zeros(n, dtype=torch.uint8).pin_memory()]
+    pb, pi, po = d.decode_host(pin[0].numpy(), 30, out=pin[1].numpy(), iters=pin[2].numpy(), ok=pin[3].numpy())
+    assert np.array_equal(pb, bits) and np.array_equal(pi, it) and np.array_equal(po, ok)
+    # pinned input, pageable outputs
+    qb, qi, qo = d.decode_host(pin[0].numpy(), 30)
+    assert np.array_equal(qb, bits) and np.array_equal(qi, it) and np.array_equal(qo, ok)
 
 
 @pytest.mark.parametrize("short,rate,es,crate", [(0, "4_5", 4.7, None), (0, "5_6", 5.2, None), (0, "8_9", 6.2, None),

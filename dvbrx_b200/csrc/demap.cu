@@ -17,6 +17,14 @@
  * multiply-adds (AVX2, AVX-512); its SSE2 build rounds the two products
  * separately and can differ by one unit on rare ties.
  *
+ * Constellations of 64 to 256 points take the minima by groups of 16 points
+ * (the four low label bits inside a group, the high ones from the groups'
+ * minima; a minimum does not depend on its order, so the LLRs are the full
+ * search's).  The 256APSK tables made of 8 rings of the same 32 phases take
+ * the reference's ring metric instead (demap.c:447-496), whose minima equal
+ * the full search's only up to rounding: c_j (-2 R_r) + R_r^2 with c_j the
+ * projection of the symbol on phase j.
+ *
  * Grid rows walk the frames, threads take four consecutive symbols (16-byte
  * loads, 4-byte stores per bit column); the points and their constants are
  * kernel parameters (constant bank).
@@ -39,6 +47,10 @@ struct DemapParams {
     int bits, nsym, nldpc, qpsk;
     int order[8];
     float ar[256], ai[256], e[256]; /* -2 re, -2 im, |p|^2 */
+    /* 256-point constellations made of 8 rings of the same 32 phases (ring in
+     * the high label bits): unit phase vectors (rc, rs), -2 R and R^2 */
+    int ring;
+    float rc[32], rs[32], rm2[8], rr2[8];
     const float* sym;
     size_t sym_stride; /* floats per frame */
     const float* n0;   /* per frame */
@@ -67,15 +79,99 @@ __device__ __forceinline__ void demap_symbol(const DemapParams& p, float x, floa
 #pragma unroll
     for (int b = 0; b < BITS; b++)
         m0[b] = m1[b] = INFINITY;
-#pragma unroll 8
-    for (int q = 0; q < (1 << BITS); q++) {
-        const float d = fmaf(x, p.ar[q], fmaf(y, p.ai[q], p.e[q]));
+    bool done = false;
+    if constexpr (BITS == 8) {
+        if (p.ring) {
+            done = true;
+        /* ring constellations (demap.c:447-496): the metric of ring r, phase j
+         * is c_j (-2 R_r) + R_r^2 with c_j = x rc_j + y rs_j; the phase bits
+         * take the minimum over rings of each phase, the ring bits the metric
+         * at the largest projection */
+        float cmax = -INFINITY;
 #pragma unroll
-        for (int b = 0; b < BITS; b++) {
-            if ((q >> (BITS - 1 - b)) & 1)
-                m1[b] = fminf(m1[b], d);
-            else
-                m0[b] = fminf(m0[b], d);
+        for (int j = 0; j < 32; j++) {
+            const float c = fmaf(x, p.rc[j], __fmul_rn(y, p.rs[j]));
+            cmax = fmaxf(cmax, c);
+            float a = fmaf(c, p.rm2[0], p.rr2[0]);
+#pragma unroll
+            for (int r = 1; r < 8; r++)
+                a = fminf(a, fmaf(c, p.rm2[r], p.rr2[r]));
+#pragma unroll
+            for (int L = 0; L < 5; L++) {
+                float& m = (j >> L) & 1 ? m1[BITS - 1 - L] : m0[BITS - 1 - L];
+                m = fminf(m, a);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const float v = fmaf(cmax, p.rm2[r], p.rr2[r]);
+#pragma unroll
+            for (int L = 5; L < 8; L++) {
+                float& m = (r >> (L - 5)) & 1 ? m1[BITS - 1 - L] : m0[BITS - 1 - L];
+                m = fminf(m, v);
+            }
+        }
+        }
+    }
+    if constexpr (BITS >= 6) {
+        if (!done) {
+        /* 64 to 256 points by groups of 16 (the minimum is order-free, so the
+         * result is the full search's): the four low label bits from a tree
+         * inside the group, the high bits from the groups' minima */
+        float gmin[1 << (BITS - 4)];
+#pragma unroll 1
+        for (int g = 0; g < (1 << (BITS - 4)); g++) {
+            float v[16];
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const int pt = 16 * g + q;
+                v[q] = fmaf(x, p.ar[pt], fmaf(y, p.ai[pt], p.e[pt]));
+            }
+            float t[16];
+#pragma unroll
+            for (int q = 0; q < 16; q++)
+                t[q] = v[q];
+#pragma unroll
+            for (int L = 0, n = 16; L < 4; L++, n /= 2) {
+                float lo = t[0], hi = t[1];
+#pragma unroll
+                for (int q = 2; q < n; q += 2) {
+                    lo = fminf(lo, t[q]);
+                    hi = fminf(hi, t[q + 1]);
+                }
+                m0[BITS - 1 - L] = fminf(m0[BITS - 1 - L], lo);
+                m1[BITS - 1 - L] = fminf(m1[BITS - 1 - L], hi);
+#pragma unroll
+                for (int q = 0; q < n / 2; q++)
+                    t[q] = fminf(t[2 * q], t[2 * q + 1]);
+            }
+            gmin[g] = t[0];
+        }
+#pragma unroll
+        for (int L = 4; L < BITS; L++) {
+            float lo = INFINITY, hi = INFINITY;
+#pragma unroll
+            for (int g = 0; g < (1 << (BITS - 4)); g++) {
+                if ((g >> (L - 4)) & 1)
+                    hi = fminf(hi, gmin[g]);
+                else
+                    lo = fminf(lo, gmin[g]);
+            }
+            m0[BITS - 1 - L] = lo;
+            m1[BITS - 1 - L] = hi;
+        }
+        }
+    } else {
+#pragma unroll 8
+        for (int q = 0; q < (1 << BITS); q++) {
+            const float d = fmaf(x, p.ar[q], fmaf(y, p.ai[q], p.e[q]));
+#pragma unroll
+            for (int b = 0; b < BITS; b++) {
+                if ((q >> (BITS - 1 - b)) & 1)
+                    m1[b] = fminf(m1[b], d);
+                else
+                    m0[b] = fminf(m0[b], d);
+            }
         }
     }
 #pragma unroll
@@ -227,6 +323,15 @@ cudaError_t launch_demap(const DemapParams& p, int sms, cudaStream_t s)
     case 5:
         k_demap<5><<<grid, 256, 0, s>>>(p);
         break;
+    case 6:
+        k_demap<6><<<grid, 256, 0, s>>>(p);
+        break;
+    case 7:
+        k_demap<7><<<grid, 256, 0, s>>>(p);
+        break;
+    case 8:
+        k_demap<8><<<grid, 256, 0, s>>>(p);
+        break;
     default:
         return cudaErrorInvalidValue;
     }
@@ -248,8 +353,8 @@ drx_demapper* drx_demapper_new(const char* constellation, const char* rate, int 
         if (!strcmp(cg_consts[i].name, constellation) && !strcmp(cg_consts[i].rate, rate) &&
             cg_consts[i].short_frame == (short_frame ? 1 : 0))
             row = &cg_consts[i];
-    if (!row || (row->order[0] >= 0 && (row->bits < 3 || row->bits > 5))) {
-        set_error(std::string("drx_demapper_new: no DVB-S2 constellation ") + constellation + " " + rate);
+    if (!row || (row->order[0] >= 0 && (row->bits < 3 || row->bits > 8))) {
+        set_error(std::string("drx_demapper_new: no DVB-S2/S2X constellation ") + constellation + " " + rate);
         return nullptr;
     }
     drx_demapper* m = new drx_demapper();
@@ -265,11 +370,36 @@ drx_demapper* drx_demapper_new(const char* constellation, const char* rate, int 
     for (int i = 0; i < np; i++)
         e += (double)row->points[2 * i] * row->points[2 * i] + (double)row->points[2 * i + 1] * row->points[2 * i + 1];
     const float g = (float)(1.0 / sqrt(e / np));
+    float pre[256], pim[256];
     for (int i = 0; i < np; i++) {
         const float re = row->points[2 * i] * g, im = row->points[2 * i + 1] * g;
+        pre[i] = re;
+        pim[i] = im;
         p.ar[i] = -2.0f * re;
         p.ai[i] = -2.0f * im;
         p.e[i] = fmaf(re, re, im * im);
+    }
+    /* 8 rings of the same 32 phases, the ring in the high label bits
+     * (demap.c:136-162): ring radii, unit phase vectors, and the check that
+     * every point is radius times phase */
+    p.ring = 0;
+    if (row->bits == 8) {
+        for (int r = 0; r < 8; r++) {
+            const float R = hypotf(pre[r << 5], pim[r << 5]);
+            p.rm2[r] = -2.0f * R;
+            p.rr2[r] = R * R;
+        }
+        const float R0 = hypotf(pre[0], pim[0]);
+        for (int j = 0; j < 32; j++) {
+            p.rc[j] = pre[j] / R0;
+            p.rs[j] = pim[j] / R0;
+        }
+        bool ring = true;
+        for (int i = 0; i < 256 && ring; i++) {
+            const float R = -0.5f * p.rm2[i >> 5];
+            ring = fabsf(R * p.rc[i & 31] - pre[i]) <= 1e-5f && fabsf(R * p.rs[i & 31] - pim[i]) <= 1e-5f;
+        }
+        p.ring = ring ? 1 : 0;
     }
     if (!cuda_check(cudaGetDevice(&m->device), "cudaGetDevice") ||
         !cuda_check(cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, m->device), "attribute") ||

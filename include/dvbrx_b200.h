@@ -308,7 +308,8 @@ int drx_bch_encode_device(drx_bch* b, uint8_t* cw, size_t stride, int nframes, v
  * int8 LLRs in codeword order, 2/n0 x (min distance, bit 1 - min distance,
  * bit 0) quantised as the reference does, the MODCOD's bit interleaver
  * applied.  Results equal drx_demap_frame of the reference's builds with
- * fused multiply-adds (AVX2, AVX-512).  DVB-S2 QPSK, 8PSK, 16APSK, 32APSK.
+ * fused multiply-adds (AVX2, AVX-512).  Every DVB-S2 and S2X constellation
+ * of the reference (QPSK to 256APSK, 128APSK with its padding bits).
  * Separate names from the reference's drx_demap_* (whose handle also serves
  * its hard-decision and noise-estimation calls): no counterpart to replace. */
 typedef struct drx_demapper drx_demapper;

@@ -1,7 +1,7 @@
 """The GPU soft demapper (drx_demapper_*) against the reference's
 drx_demap_frame (demap.c) compiled from its sources: identical int8 LLRs for
-the DVB-S2 constellations on normal and short frames, at saturating and
-noisy Es/N0, and chained into the LDPC decoder.  Exactness holds for the
+the DVB-S2 and S2X constellations on normal and short frames, at saturating
+and noisy Es/N0, and chained into the LDPC decoder.  Exactness holds for the
 reference's builds with fused multiply-adds (AVX2, AVX-512); its SSE2 build
 may differ by one unit on rare ties."""
 import ctypes
@@ -17,7 +17,13 @@ from oracle import datagen
 pytestmark = pytest.mark.gpu
 
 CASES = [("QPSK", "1_2", 0), ("QPSK", "8_9", 1), ("8PSK", "3_5", 0), ("8PSK", "2_3", 1), ("16APSK", "2_3", 0),
-         ("16APSK", "8_9", 1), ("32APSK", "3_4", 0), ("32APSK", "9_10", 0), ("32APSK", "5_6", 1)]
+         ("16APSK", "8_9", 1), ("32APSK", "3_4", 0), ("32APSK", "9_10", 0), ("32APSK", "5_6", 1),
+         # DVB-S2X: 8 to 256 points; 128APSK pads 6 bits; the 256APSK tables made of 8 rings of the
+         # same 32 phases take the reference's ring metric, the others the full search
+         ("8APSK", "100_180", 0), ("8_8APSK", "90_180", 0), ("4_12_16APSK", "32_45", 1),
+         ("4_8_4_16APSK", "128_180", 0), ("64APSK", "128_180", 0), ("8_16_20_20APSK", "7_9", 0),
+         ("4_12_20_28APSK", "132_180", 0), ("128APSK", "135_180", 0), ("256APSK", "116_180", 0),
+         ("256APSK", "135_180", 0), ("256APSK", "20_30", 0), ("256APSK", "22_30", 0)]
 
 
 def ref_demap(const, rate, short, sym_iq, n0):

@@ -16,6 +16,13 @@ hand-written forward and backward kernels (learned.LearnedMinSum).
 The exported table (JSON: scale and offset [iters][classes], the class of
 every check degree) is what Ldpc.set_learned / drx_ldpc_set_learned load;
 the int8 decoders round it to Q8.
+
+Data-parallel on several GPUs (one process per GPU, torchrun): every rank
+draws its own minibatches (a rank-dependent seed) and the gradient of the
+tables, a few hundred numbers, is averaged with one all-reduce per step, so
+the ranks keep identical tables; rank 0 logs and writes the table.
+
+    torchrun --nproc-per-node 8 -m dvbrx_b200.train --rate 3_5 --const 8PSK ...
 """
 import argparse
 import json
@@ -30,6 +37,38 @@ from . import FecParams, Ldpc, code_info, fec_lookup
 from .learned import LearnedDecoder, degree_classes, learned_posteriors
 
 TABLES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "learned_tables")
+
+
+def dist_world():
+    """(world size, rank) of the initialised process group, (1, 0) without one."""
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_world_size(), dist.get_rank()
+    return 1, 0
+
+
+def rank_seed(seed, rank):
+    """Minibatch seed of a rank: distinct frames on every rank."""
+    return seed + 1000003 * rank
+
+
+def average_gradients(params, world):
+    """Mean of every parameter's gradient over the ranks, in one all-reduce
+    of the flattened gradients (the learned tables are small)."""
+    import torch.distributed as dist
+
+    grads = [p.grad for p in params if p.grad is not None]
+    if world <= 1 or not grads:
+        return
+    flat = torch.cat([g.reshape(-1) for g in grads])
+    dist.all_reduce(flat)
+    flat /= world
+    k = 0
+    for g in grads:
+        n = g.numel()
+        g.copy_(flat[k:k + n].view_as(g))
+        k += n
 
 
 def table_path(short_frame, rate, constellation, iters):
@@ -118,8 +157,9 @@ def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, l
           weights="uniform", val_points=None):
     """Adam on the fp32 masters of the FP16 tables, initialised to the
     plain decoder (scale 1, offset 1).  Returns (model, history)."""
+    world, rank = dist_world()
     torch.manual_seed(seed)
-    rng = np.random.default_rng(seed)
+    rng = np.random.default_rng(rank_seed(seed, rank))
     model = LearnedDecoder(short_frame, rate, iters=iters, params=_params(short_frame, rate),
                            weights=loss_weights(weights, iters))
     vset = validation_set(model.dec, val_points or [es_lo, (es_lo + es_hi) / 2, es_hi], 256, constellation)
@@ -135,6 +175,7 @@ def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, l
         loss = model(llr16, info)
         opt.zero_grad()
         loss.backward()
+        average_gradients(list(model.parameters()), world)
         opt.step()
         with torch.no_grad():
             model.beta.clamp_(0.0, 4.0)
@@ -227,7 +268,13 @@ def main(argv=None):
                          "[QEF - 0.25, QEF + 0.75] dB, into --out-dir")
     ap.add_argument("--out-dir", default=None)
     a = ap.parse_args(argv)
-    log = lambda s: print(s, flush=True)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl")
+    world, rank = dist_world()
+    log = (lambda s: print(s, flush=True)) if rank == 0 else (lambda s: None)
     if a.all_s2:
         from .modcods import RATES, qef_db
         out_dir = a.out_dir or TABLES
@@ -251,8 +298,9 @@ def main(argv=None):
                         "train_wall_s": time.time() - t0}
                 table = export(model, meta)
                 path = os.path.join(out_dir, os.path.basename(table_path(short, rate, "QPSK", a.iters)))
-                with open(path, "w") as f:
-                    json.dump(table, f, indent=1)
+                if rank == 0:
+                    with open(path, "w") as f:
+                        json.dump(table, f, indent=1)
                 log(json.dumps({"table": os.path.basename(path), "wall_s": meta["train_wall_s"],
                                 "validation": model.validation}))
                 del model
@@ -278,12 +326,19 @@ def main(argv=None):
             "loss_first": hist[0]["loss"], "loss_last": float(np.mean([h["loss"] for h in hist[-10:]])),
             "train_ms_per_step": float(np.median(ms)), "train_frames_per_s": a.batch / (float(np.median(ms)) * 1e-3),
             "train_wall_s": wall}
+    meta["ranks"] = world
     table = export(model, meta)
     out = a.out or table_path(a.short, a.rate, a.const, a.iters)
-    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
-    with open(out, "w") as f:
-        json.dump(table, f, indent=1)
+    if rank == 0:
+        os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+        with open(out, "w") as f:
+            json.dump(table, f, indent=1)
     log(json.dumps({k: v for k, v in meta.items()}))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 

@@ -76,3 +76,46 @@ def test_missing_rank_times_out():
     msg = q.get(timeout=120)
     p.join(timeout=60)
     assert msg.startswith("error"), msg
+
+
+def _grad_rank(rank, world, port, q):
+    sys.path.insert(0, ROOT)
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    import torch
+    import torch.distributed as dist
+
+    from dvbrx_b200 import train
+    dist.init_process_group("gloo", world_size=world, rank=rank, timeout=__import__("datetime").timedelta(seconds=30))
+    w, r = train.dist_world()
+    # two parameters shaped like the learned tables, rank-dependent gradients
+    a = torch.zeros(12, 4, requires_grad=True)
+    b = torch.zeros(12, 4, requires_grad=True)
+    (a * (r + 1)).sum().backward()
+    (b * (2 * r + 3)).sum().backward()
+    train.average_gradients([a, b], w)
+    seeds = [train.rank_seed(7, r)]
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((r, w, float(a.grad.mean()), float(b.grad.mean()), float(a.grad.std()), seeds))
+
+
+def test_training_gradients_averaged_over_ranks():
+    """Data-parallel training: one all-reduce gives every rank the mean
+    gradient of the learned tables (so the tables stay identical), and the
+    ranks draw different minibatches."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_grad_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, w0, a0, b0, s0, seed0), (r1, w1, a1, b1, s1, seed1) = res
+    assert (w0, w1) == (2, 2)
+    assert a0 == a1 == 1.5 and b0 == b1 == 4.0  # means of (1, 2) and (3, 5)
+    assert s0 == s1 == 0.0
+    assert seed0 != seed1

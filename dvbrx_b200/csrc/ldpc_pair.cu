@@ -403,16 +403,21 @@ __device__ void load_lane(const DevCode& c, const PairFrame& fr, const int8_t* _
 
 /* Syndrome of both lanes: bit h of the result set if lane h fails.  Thread
  * t checks column t % 360 of every other layer; the scan stops once both
- * lanes have failed. */
-__device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int* sflag)
+ * lanes have failed.  The result is the OR over all layers, so the scan may
+ * start anywhere: it starts at a layer where the previous scan found a
+ * failure (srow[0], fixed during a scan; srow[1] collects a failing layer),
+ * which a frame that still fails usually fails again. */
+__device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int* sflag, volatile int* srow)
 {
     const int t = threadIdx.x;
     const int nh = blockDim.x / kQCp; /* threads per column */
+    const int i0 = srow[0];
     int fail = 0;
     if (t < nh * kQCp) {
         const int j = t % kQCp, h0 = t / kQCp;
         const uint16_t* post = fr.post;
-        for (int i = h0; i < c.q; i += nh) {
+        for (int k = h0; k < c.q; k += nh) {
+            const int i = k + i0 < c.q ? k + i0 : k + i0 - c.q;
             if (*sflag == 3)
                 break;
             const uint32_t pc = sx2(post[c.K + kQCp * i + j]);
@@ -432,11 +437,14 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
             if (f & ~fail) {
                 fail |= f;
                 atomicOr((int*)sflag, f);
+                srow[1] = i;
             }
         }
     }
     __syncthreads();
     const int r = *sflag;
+    if (t == 0)
+        srow[0] = srow[1];
     __syncthreads();
     return r;
 }
@@ -608,7 +616,7 @@ template <int A, int B, int GDM, int LS>
 __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
 {
     extern __shared__ __align__(16) char smem[];
-    __shared__ int s_frame[2], s_iter[2], s_flag, s_reload;
+    __shared__ int s_frame[2], s_iter[2], s_flag, s_reload, s_row[2];
     const DevCode c = *p.code;
     const PairFrame fr = stage_pair(c, smem);
     const int lT = stage_learn(p.learn, p.learn_class, p.learn_iters);
@@ -619,6 +627,7 @@ __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
         s_frame[0] = s_frame[1] = -1;
         s_flag = 0;
         s_reload = 3;
+        s_row[0] = s_row[1] = 0;
     }
     __syncthreads();
     if (p.group > 0) {
@@ -644,7 +653,7 @@ __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
             int it = 0;
             bool ok = true;
             for (;;) {
-                const int fail = syndrome_pair(c, fr, &s_flag);
+                const int fail = syndrome_pair(c, fr, &s_flag, s_row);
                 if (t == 0)
                     s_flag = 0; /* read again only after later barriers */
                 const int v = pair_team_vote(sync + 2 * it, M, fail != 0, p.err);
@@ -697,7 +706,7 @@ __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
         }
         if (s_frame[0] < 0 && s_frame[1] < 0)
             break;
-        const int fail = syndrome_pair(c, fr, &s_flag);
+        const int fail = syndrome_pair(c, fr, &s_flag, s_row);
         /* lanes whose frame is done: results out, refill */
         int done = 0;
         for (int h = 0; h < 2; h++) {

@@ -16,14 +16,18 @@ pytestmark = pytest.mark.gpu
 _handles = {}
 
 
+def fec_params(short, rate):
+    try:
+        return D.fec_lookup(short, rate)
+    except KeyError:  # T2 codes: no BCH row, nbch = K
+        info = D.code_info(short, rate)
+        return D.FecParams(short, info.nldpc, info.K, info.K, 0)
+
+
 def handle(short, rate, kldpc=None):
     key = (short, rate, kldpc)
     if key not in _handles:
-        try:
-            p = D.fec_lookup(short, rate)
-        except KeyError:  # T2 codes: no BCH row, nbch = K
-            info = D.code_info(short, rate)
-            p = D.FecParams(short, info.nldpc, info.K, info.K, 0)
+        p = fec_params(short, rate)
         if kldpc is not None:
             p.kldpc = kldpc
         _handles[key] = D.Ldpc(p, rate)
@@ -281,4 +285,36 @@ def test_pair_matches_frame_high_degree(short, rate, es, crate):
         assert np.array_equal(a, b), rate
     it, ok = out[D.VARIANT_PAIR][1], out[D.VARIANT_PAIR][2]
     assert 0 < ok.sum() and it.max() > 3, "the case should have converging frames that need iterations"
+    d.close()
+
+
+@pytest.mark.parametrize("short,rate", RATES)
+def test_pair_matches_frame_every_code(short, rate):
+    """Every code of both frame sizes: on 256 frames near the waterfall the
+    frame-pair kernel gives the one-frame kernel's bits, iterations and flags,
+    with per-frame stopping and with group stopping (64-frame groups)."""
+    import re
+
+    import torch
+
+    d = D.Ldpc(fec_params(short, rate), rate)
+    if rate in SNR:
+        es = SNR[rate]
+    else:
+        m = re.match(r"(\d+)_(\d+)", rate)
+        es = 10 * np.log10(2 ** (2 * int(m.group(1)) / int(m.group(2))) - 1) + 0.8
+    try:
+        llr, _, _ = d.generate(256, float(es), seed=zlib.crc32(rate.encode()) + 7 * short, constellation="QPSK")
+    except RuntimeError:
+        # no QPSK MODCOD of this code: QPSK with the 1/2 mapping stands in
+        llr, _, _ = d.generate(256, float(es), seed=zlib.crc32(rate.encode()) + 7 * short, constellation="QPSK",
+                               const_rate="1_2")
+    host = llr.cpu().numpy()[:128]
+    res = {}
+    for v in (D.VARIANT_FRAME, D.VARIANT_PAIR):
+        assert d.set_variant(v) == v
+        res[v] = [t.cpu().numpy() for t in d.decode_device(llr, 30)] + list(d.decode_host(host, 30, stop=64))
+    torch.cuda.synchronize()
+    for a, b in zip(res[D.VARIANT_FRAME], res[D.VARIANT_PAIR]):
+        assert np.array_equal(a, b), rate
     d.close()

@@ -137,3 +137,31 @@ def test_learned_words_rounding():
     assert w[0, 1] & 0xFFFF == 0 and (w[0, 1] >> 16) == (0x10000 - 128)  # 0.5 -> 0 (half-even), -0.5 -> -128
     assert w[0, 2] & 0xFFFF == 65535 and (w[0, 2] >> 16) == 32767
     assert w[0, 3] & 0xFFFF == 0 and (w[0, 3] >> 16) == 0x8000
+
+
+@needs_ref
+@pytest.mark.parametrize("short,rates", [(0, ["1_4", "3_5", "9_10"]), (1, ["1_4", "1_2", "8_9"])])
+def test_bch_encoder_matches_reference_decoder(short, rates):
+    """The oracle's BCH encoder (both fields, every t) makes words the
+    reference's bch.c accepts with no correction; with t errors planted it
+    corrects exactly t bits back to the codeword, and with t + 1 it never
+    returns the codeword."""
+    rng = np.random.default_rng(17 + short)
+    for rate in rates:
+        p = oracle.fec_params(short, rate)
+        msgs = np.packbits(rng.integers(0, 2, (3, p.kbch), dtype=np.uint8), axis=1)
+        cw = oracle.bch_encode(short, rate, msgs)
+        assert np.array_equal(np.unpackbits(cw, axis=1)[:, : p.kbch], np.unpackbits(msgs, axis=1)[:, : p.kbch])
+        ref = oracle.RefBch(short, rate)
+        w, r = ref.decode(cw)
+        assert (r == 0).all() and np.array_equal(w, cw), rate
+        for wgt in (p.t, p.t + 1):
+            bad = cw.copy()
+            for f in range(bad.shape[0]):
+                for b in rng.choice(p.kldpc, wgt, replace=False):
+                    bad[f, b // 8] ^= 0x80 >> (b % 8)
+            w, r = ref.decode(bad)
+            if wgt == p.t:
+                assert (r == p.t).all() and np.array_equal(w, cw), rate
+            else:
+                assert not any(np.array_equal(w[f], cw[f]) for f in range(w.shape[0])), rate

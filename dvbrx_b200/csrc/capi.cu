@@ -591,9 +591,23 @@ drx_ldpc* drx_ldpc_new(const drx_fec_params* p, const char* rate)
     d->ctas_per_sm = decode_ctas_per_sm(d->code.dclass, d->smem);
     d->pair_kid = pair_kernel_id(d->code);
     if (d->pair_kid >= 0) {
-        d->pair_smem = decode_pair_smem_bytes(d->code.N, (int)d->code.ent.size() / 2,
-                                              (int)d->code.steps.size(), d->code.q);
+        auto smem_of = [&](int kid) {
+            return decode_pair_smem_bytes(d->code.N, d->code.K, (int)d->code.ent.size() / 2,
+                                          (int)d->code.steps.size(), d->code.q, kid);
+        };
+        d->pair_smem = smem_of(d->pair_kid);
         d->pair_ctas_per_sm = decode_pair_ctas_per_sm(d->pair_kid, d->pair_smem);
+        /* the parity-out twin when it makes more CTAs resident */
+        const int po = pair_kernel_po_twin(d->pair_kid);
+        if (po >= 0) {
+            const size_t sm = smem_of(po);
+            const int n = decode_pair_ctas_per_sm(po, sm);
+            if (n > d->pair_ctas_per_sm) {
+                d->pair_kid = po;
+                d->pair_smem = sm;
+                d->pair_ctas_per_sm = n;
+            }
+        }
     }
     if (d->ctas_per_sm <= 0) {
         set_err("decoder kernel does not fit on this device");

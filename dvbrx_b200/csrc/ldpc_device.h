@@ -143,7 +143,11 @@ namespace drxg {
  * instantiation for a code (-1: not run by the frame-pair kernel). */
 struct Code;
 int pair_kernel_id(const Code& c);
-size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q);
+/* The parity-out twin of kernel kid (parity posteriors in the CTA's global
+ * slab and registers, about half the shared memory, two CTAs per SM), -1 if
+ * it has none */
+int pair_kernel_po_twin(int kid);
+size_t decode_pair_smem_bytes(int N, int K, int nent, int nsteps, int q, int kid);
 size_t decode_pair_msg_bytes(int R, int kid);
 int decode_pair_ctas_per_sm(int kid, size_t smem);
 cudaError_t launch_decode_pair(const DecodeParams& p, int kid, size_t smem, int grid, cudaStream_t stream);

@@ -109,8 +109,10 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
 template <bool WIDE>
 using PairRec = typename std::conditional<WIDE, uint4, uint2>::type;
 
-/* WIDE: the kernel's records are 16 bytes (its degree bound is above 16) */
-template <int DM, bool EXACT, int LS, bool WIDE>
+/* WIDE: the kernel's records are 16 bytes (its degree bound is above 16).
+ * PO: the parity posteriors (slots 0 and 1) are not in shared memory; the
+ * layer loop hands their two-byte words in and takes the new ones back. */
+template <int DM, bool EXACT, int LS, bool WIDE, bool PO>
 struct PairCheck {
     static_assert(DM <= (WIDE ? 32 : 16), "degree above the record's slots");
     using Rec = PairRec<WIDE>;
@@ -140,7 +142,7 @@ struct PairCheck {
 #pragma unroll
         for (int k = 0; k < S; k++) {
             if (k < 2) {
-                addr[k] = sbase + 2u * (uint32_t)(k == 0 ? pc : pp);
+                addr[k] = PO ? 0u : sbase + 2u * (uint32_t)(k == 0 ? pc : pp);
             } else {
                 /* a slot past the degree takes the last link's address: read, never used */
                 const int2 e = ent[min(k, D - 1) - 2];
@@ -189,14 +191,15 @@ struct PairCheck {
      * slots; otherwise only the slots that can be absent are masked (the
      * previous parity of check (0, 0)). */
     template <bool LEV>
-    __device__ __forceinline__ void read_all(const uint16_t* __restrict__ post)
+    __device__ __forceinline__ void read_all(const uint16_t* __restrict__ post, uint32_t r0, uint32_t r1)
     {
         const uint32_t excl = LEV ? (~live | inm) : ~live;
         uint32_t f[S];
 #pragma unroll
         for (int k = 0; k < S; k++) {
             const uint32_t m = unmsg(k);
-            uint32_t v = sadd(sx2(lds16(addr[k])), m);
+            const uint32_t raw = PO && k < 2 ? (k == 0 ? r0 : r1) : lds16(addr[k]);
+            uint32_t v = sadd(sx2(raw), m);
             if (LEV || !EXACT || k == 1)
                 v = ((excl >> k) & 1u) ? 0x00FF00FFu : v;
             f[k] = v;
@@ -302,8 +305,9 @@ struct PairCheck {
 
     /* every other posterior (predicated stores) and the node's compressed
      * messages for both lanes, stored by thread 0: the slot holding min0 and
-     * one sign bit per slot */
-    __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, Rec* __restrict__ dst)
+     * one sign bit per slot.  PO: the parity words go to o0 and o1. */
+    __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, Rec* __restrict__ dst, uint32_t& o0,
+                                               uint32_t& o1)
     {
         const uint32_t wm = live & ~outm;
         uint32_t nidx = 0, nsg = 0, nsg1 = 0; /* nidx per lane: k + 1 of a slot holding min0, 0 if none */
@@ -311,7 +315,9 @@ struct PairCheck {
         for (int k = 0; k < S; k++) {
             uint32_t above, neg;
             const uint32_t nv = update(k, above, neg);
-            if ((wm >> k) & 1u)
+            if (PO && k < 2)
+                (k == 0 ? o0 : o1) = nv;
+            else if ((wm >> k) & 1u)
                 sts16(addr[k], nv);
             nidx = sel(above, nidx, (uint32_t)(k + 1) * 0x00010001u);
             if (k < 16)
@@ -333,15 +339,27 @@ struct PairFrame {
     const int2* ent; /* (shared byte address of the link for check 0 before the wrap, a) */
     const uint16_t* eoff;
     const uint32_t* steps;
+    /* parity out of shared memory (PO kernels): the posterior word of
+     * parity bit (i, j) is gpar[360 i + j] (global, this CTA's slab) for
+     * i < q - 1 and wrap[j] (shared) for the last layer */
+    uint16_t* gpar;
+    uint16_t* wrap;
 };
 
 __device__ __forceinline__ size_t a16p(size_t v) { return (v + 15) & ~(size_t)15; }
 
-__device__ PairFrame stage_pair(const DevCode& c, char* smem)
+template <bool PO>
+__device__ PairFrame stage_pair(const DevCode& c, char* smem, uint16_t* gpar)
 {
     PairFrame f;
     f.post = (uint16_t*)smem;
-    size_t off = a16p(2 * (size_t)c.N);
+    size_t off = a16p(2 * (size_t)(PO ? c.K : c.N));
+    f.gpar = gpar;
+    f.wrap = nullptr;
+    if (PO) {
+        f.wrap = (uint16_t*)(smem + off);
+        off += a16p(2 * (size_t)kQCp);
+    }
     int2* ent = (int2*)(smem + off);
     off += a16p(sizeof(int2) * c.nent);
     uint16_t* eoff = (uint16_t*)(smem + off);
@@ -364,15 +382,27 @@ __device__ PairFrame stage_pair(const DevCode& c, char* smem)
     return f;
 }
 
+/* Byte `h` of the posterior word of parity bit (ii, jj) */
+template <bool PO>
+__device__ __forceinline__ uint8_t* parity_byte(const DevCode& c, const PairFrame& fr, uint32_t ii, uint32_t jj, int h)
+{
+    if (!PO)
+        return (uint8_t*)fr.post + 2 * (c.K + kQCp * ii + jj) + h;
+    return ii + 1 < (uint32_t)c.q ? (uint8_t*)fr.gpar + 2 * (kQCp * ii + jj) + h : (uint8_t*)fr.wrap + 2 * jj + h;
+}
+
 /* Frame f's LLRs into byte `h` of every posterior word (f < 0: the all-zero
  * codeword at full confidence, which passes every check). */
+template <bool PO>
 __device__ void load_lane(const DevCode& c, const PairFrame& fr, const int8_t* __restrict__ src, int h)
 {
     uint8_t* b = (uint8_t*)fr.post + h;
     const int t = threadIdx.x;
     if (!src) {
-        for (int v = t; v < c.N; v += blockDim.x)
+        for (int v = t; v < c.K; v += blockDim.x)
             b[2 * v] = 127;
+        for (int k = t; k < c.R; k += blockDim.x)
+            *parity_byte<PO>(c, fr, k / kQCp, k % kQCp, h) = 127;
         return;
     }
     if (((uintptr_t)src & 7) == 0) {
@@ -390,14 +420,14 @@ __device__ void load_lane(const DevCode& c, const PairFrame& fr, const int8_t* _
             for (int r = 0; r < 8; r++) {
                 const uint32_t k = 8u * u + r;
                 const uint32_t jj = __umulhi(k, qm), ii = k - jj * c.q;
-                b[2 * (c.K + kQCp * ii + jj)] = (uint8_t)((r < 4 ? w.x : w.y) >> (8 * (r & 3)));
+                *parity_byte<PO>(c, fr, ii, jj, h) = (uint8_t)((r < 4 ? w.x : w.y) >> (8 * (r & 3)));
             }
         }
     } else {
         for (int v = t; v < c.K; v += blockDim.x)
             b[2 * v] = (uint8_t)src[v];
         for (int k = t; k < c.R; k += blockDim.x)
-            b[2 * (c.K + kQCp * (k % c.q) + k / c.q)] = (uint8_t)src[c.K + k];
+            *parity_byte<PO>(c, fr, k % c.q, k / c.q, h) = (uint8_t)src[c.K + k];
     }
 }
 
@@ -407,6 +437,22 @@ __device__ void load_lane(const DevCode& c, const PairFrame& fr, const int8_t* _
  * start anywhere: it starts at a layer where the previous scan found a
  * failure (srow[0], fixed during a scan; srow[1] collects a failing layer),
  * which a frame that still fails usually fails again. */
+/* The posterior words of the two parity bits of check (i, j): its own and
+ * the previous one (for check (0, 0), none: a positive stand-in) */
+template <bool PO>
+__device__ __forceinline__ void parity_words(const DevCode& c, const PairFrame& fr, int i, int j, uint32_t& pc,
+                                             uint32_t& pp)
+{
+    if (PO) {
+        pc = i + 1 < c.q ? fr.gpar[kQCp * i + j] : fr.wrap[j];
+        pp = i ? fr.gpar[kQCp * (i - 1) + j] : (j ? fr.wrap[j - 1] : 0x0101u);
+    } else {
+        pc = fr.post[c.K + kQCp * i + j];
+        pp = i ? fr.post[c.K + kQCp * (i - 1) + j] : (j ? fr.post[c.K + kQCp * (c.q - 1) + j - 1] : 0x0101u);
+    }
+}
+
+template <bool PO>
 __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int* sflag, volatile int* srow)
 {
     const int t = threadIdx.x;
@@ -415,29 +461,45 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
     int fail = 0;
     if (t < nh * kQCp) {
         const int j = t % kQCp, h0 = t / kQCp;
-        const uint16_t* post = fr.post;
-        for (int k = h0; k < c.q; k += nh) {
-            const int i = k + i0 < c.q ? k + i0 : k + i0 - c.q;
-            if (*sflag == 3)
-                break;
-            const uint32_t pc = sx2(post[c.K + kQCp * i + j]);
-            const uint32_t pp = i ? sx2(post[c.K + kQCp * (i - 1) + j])
-                                  : (j ? sx2(post[c.K + kQCp * (c.q - 1) + j - 1]) : 0x00010001u);
-            uint32_t par = pc ^ pp;
-            uint32_t z = (__vadd2(pc, 0xFFFFFFFFu) & ~pc) | (__vadd2(pp, 0xFFFFFFFFu) & ~pp);
-            const int e1 = fr.eoff[i + 1];
-            for (int e = fr.eoff[i]; e < e1; e++) {
-                const int2 en = fr.ent[e];
-                const uint32_t v = sx2(lds16((uint32_t)en.x + 2u * (uint32_t)j + (j < en.y ? 2u * kQCp : 0u)));
-                par ^= v;
-                z |= __vadd2(v, 0xFFFFFFFFu) & ~v;
-            }
-            const uint32_t bad = (par | z);
-            const int f = ((bad >> 15) & 1) | ((bad >> 30) & 2);
-            if (f & ~fail) {
-                fail |= f;
-                atomicOr((int*)sflag, f);
-                srow[1] = i;
+        /* parity words are loaded D rows ahead (global memory in PO kernels) */
+        constexpr int D = 4;
+        auto row = [&](int k) { return k + i0 < c.q ? k + i0 : k + i0 - c.q; };
+        uint32_t bc[D], bp[D];
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            bc[d] = bp[d] = 0;
+            if (h0 + d * nh < c.q)
+                parity_words<PO>(c, fr, row(h0 + d * nh), j, bc[d], bp[d]);
+        }
+        bool stop = false;
+        for (int k0 = h0; k0 < c.q && !stop; k0 += D * nh) {
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+                const int k = k0 + d * nh;
+                if (k >= c.q || *sflag == 3) {
+                    stop = true;
+                    break;
+                }
+                const int i = row(k);
+                const uint32_t pc = sx2(bc[d]), pp = sx2(bp[d]);
+                if (k + D * nh < c.q)
+                    parity_words<PO>(c, fr, row(k + D * nh), j, bc[d], bp[d]);
+                uint32_t par = pc ^ pp;
+                uint32_t z = (__vadd2(pc, 0xFFFFFFFFu) & ~pc) | (__vadd2(pp, 0xFFFFFFFFu) & ~pp);
+                const int e1 = fr.eoff[i + 1];
+                for (int e = fr.eoff[i]; e < e1; e++) {
+                    const int2 en = fr.ent[e];
+                    const uint32_t v = sx2(lds16((uint32_t)en.x + 2u * (uint32_t)j + (j < en.y ? 2u * kQCp : 0u)));
+                    par ^= v;
+                    z |= __vadd2(v, 0xFFFFFFFFu) & ~v;
+                }
+                const uint32_t bad = (par | z);
+                const int f = ((bad >> 15) & 1) | ((bad >> 30) & 2);
+                if (f & ~fail) {
+                    fail |= f;
+                    atomicOr((int*)sflag, f);
+                    srow[1] = i;
+                }
             }
         }
     }
@@ -459,11 +521,11 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
  * constrain the bits two checks of a layer share, so the wavefront levels
  * carry just those links.  Unlevelled layers take one pass.
  */
-template <int DM, bool EXACT, int LS, bool WIDE, bool LEARNED>
+template <int DM, bool EXACT, int LS, bool WIDE, bool LEARNED, bool PO>
 __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev,
                                            PairRec<WIDE> rec, unsigned long long meta, uint32_t fresh,
-                                           PairRec<WIDE>* __restrict__ msg,
-                                           int lA, int lB)
+                                           PairRec<WIDE>* __restrict__ msg, int lA, int lB, uint32_t r0,
+                                           uint32_t r1, uint32_t& o0, uint32_t& o1)
 {
     const int t = threadIdx.x;
     const bool active = t < kQCp;
@@ -477,15 +539,15 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             b = s_learn_tab[lB + k];
         }
     };
-    using Ck = PairCheck<DM, EXACT, LS, WIDE>;
+    using Ck = PairCheck<DM, EXACT, LS, WIDE, PO>;
     Ck ck;
     if (active) {
         ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, rec, fresh, meta,
                  (uint32_t)__cvta_generic_to_shared(fr.post));
         if (nlev > 1)
-            ck.template read_all<true>(fr.post);
+            ck.template read_all<true>(fr.post, r0, r1);
         else
-            ck.template read_all<false>(fr.post);
+            ck.template read_all<false>(fr.post, r0, r1);
     } else {
         ck.idle((uint32_t)__cvta_generic_to_shared(fr.post));
     }
@@ -522,7 +584,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
         ck.finish(true, LEARNED, wa, wb);
     }
     if (active)
-        ck.write_rest(fr.post, msg + kQCp * i + j);
+        ck.write_rest(fr.post, msg + kQCp * i + j, o0, o1);
     __syncthreads();
 }
 
@@ -530,7 +592,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
  * level metadata are fetched one layer ahead.  The kernel is compiled for
  * the two information-link counts A <= B of its codes (exact-degree check
  * nodes), or, with GDM > 0, for any count up to GDM - 2 (predicated). */
-template <int A, int B, int GDM, int LS, bool LEARNED>
+template <int A, int B, int GDM, int LS, bool LEARNED, bool PO>
 __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, uint32_t fresh, int lA, int lB)
 {
     constexpr bool WIDE = (GDM > 0 ? GDM : B + 2) > 16;
@@ -541,26 +603,55 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, 
     const bool active = t < kQCp;
     Rec rn{};
     unsigned long long mn = 0;
+    /* PO: the word of parity bit (i, j) for layer i (loaded a layer ahead),
+     * and of (i - 1, j), which the previous layer of this thread wrote */
+    uint32_t pnext = 0, carry = 0;
     if (active) {
         rn = __ldcg(msg + j);
         mn = __ldg(c.lmeta + j);
+        if (PO && c.q > 1)
+            pnext = fr.gpar[j];
     }
     for (int i = 0; i < c.q; i++) {
         const Rec rec = rn;
         const unsigned long long meta = mn;
+        uint32_t r0 = 0, r1 = 0, o0 = 0, o1 = 0;
         if (active && i + 1 < c.q) {
             rn = __ldcg(msg + kQCp * (i + 1) + j);
             mn = __ldg(c.lmeta + kQCp * (i + 1) + j);
         }
+        if (PO && active) {
+            r0 = i + 1 < c.q ? pnext : fr.wrap[j];
+            if (i + 2 < c.q)
+                pnext = fr.gpar[kQCp * (i + 1) + j];
+            r1 = i ? carry : (j ? fr.wrap[j - 1] : 0u);
+        }
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
         const int nlev = c.nlev[i];
         if (GDM > 0)
-            layer_pair<(GDM > 0 ? GDM : 2), false, LS, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<(GDM > 0 ? GDM : 2), false, LS, WIDE, LEARNED, PO>(fr, c, i, cnt, nlev, rec, meta, fresh, msg,
+                                                                           lA, lB, r0, r1, o0, o1);
         else if (A == B || cnt == A)
-            layer_pair<A + 2, true, LS, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<A + 2, true, LS, WIDE, LEARNED, PO>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB, r0, r1,
+                                                           o0, o1);
         else
-            layer_pair<B + 2, true, LS, WIDE, LEARNED>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB);
+            layer_pair<B + 2, true, LS, WIDE, LEARNED, PO>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB, r0, r1,
+                                                           o0, o1);
+        /* (i - 1, j) is final for this iteration; (i, j) goes to the next
+         * layer, or, for the last layer, to the check (0, j + 1) */
+        if (PO && active) {
+            if (i)
+                fr.gpar[kQCp * (i - 1) + j] = (uint16_t)o1;
+            else if (j)
+                fr.wrap[j - 1] = (uint16_t)o1;
+            if (i + 1 < c.q)
+                carry = o0;
+            else
+                fr.wrap[j] = (uint16_t)o0;
+        }
     }
+    if (PO)
+        __syncthreads(); /* the last layer's wrap words before the syndrome reads them */
 }
 
 __device__ void store_lane(const DevCode& c, const PairFrame& fr, int h, uint8_t* __restrict__ dst)
@@ -612,16 +703,21 @@ __device__ int pair_team_vote(unsigned* slot, int M, bool fail, int* err)
     return r;
 }
 
-template <int A, int B, int GDM, int LS>
-__global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
+/* PO: parity posteriors out of shared memory (two CTAs per SM for normal
+ * frames up to rate 4/5); the kernel is then compiled for two resident CTAs */
+template <int A, int B, int GDM, int LS, bool PO>
+__global__ void __launch_bounds__(384, PO ? 2 : 1) k_decode_pair(DecodeParams p)
 {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_frame[2], s_iter[2], s_flag, s_reload, s_row[2];
     const DevCode c = *p.code;
-    const PairFrame fr = stage_pair(c, smem);
+    constexpr bool WIDE = (GDM > 0 ? GDM : B + 2) > 16;
+    void* msg = (char*)p.msg + (size_t)blockIdx.x * p.msg_stride;
+    /* the parity words follow the message records in this CTA's slab */
+    uint16_t* gpar = (uint16_t*)((char*)msg + (((size_t)c.R * (WIDE ? 16 : 8) + 15) & ~(size_t)15));
+    const PairFrame fr = stage_pair<PO>(c, smem, gpar);
     const int lT = stage_learn(p.learn, p.learn_class, p.learn_iters);
     const int nframes = p.nframes_dev ? *p.nframes_dev : p.nframes;
-    void* msg = (char*)p.msg + (size_t)blockIdx.x * p.msg_stride;
     const int t = threadIdx.x;
     if (t == 0) {
         s_frame[0] = s_frame[1] = -1;
@@ -646,21 +742,21 @@ __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
                 const int f = g * G + 2 * member + h;
                 fr2[h] = f < end ? f : -1;
                 const int row = fr2[h] < 0 ? 0 : p.rows ? p.rows[fr2[h]] : fr2[h];
-                load_lane(c, fr, fr2[h] >= 0 ? p.llr + (size_t)row * p.llr_stride : nullptr, h);
+                load_lane<PO>(c, fr, fr2[h] >= 0 ? p.llr + (size_t)row * p.llr_stride : nullptr, h);
             }
             __syncthreads();
             uint32_t gfresh = 0xFFFFFFFFu;
             int it = 0;
             bool ok = true;
             for (;;) {
-                const int fail = syndrome_pair(c, fr, &s_flag, s_row);
+                const int fail = syndrome_pair<PO>(c, fr, &s_flag, s_row);
                 if (t == 0)
                     s_flag = 0; /* read again only after later barriers */
                 const int v = pair_team_vote(sync + 2 * it, M, fail != 0, p.err);
                 ok = v == 1;
                 if (v < 0 || ok || it >= p.max_iter)
                     break;
-                iterate_pair<A, B, GDM, LS, false>(c, fr, msg, gfresh, -1, -1);
+                iterate_pair<A, B, GDM, LS, false, PO>(c, fr, msg, gfresh, -1, -1);
                 gfresh = 0;
                 it++;
             }
@@ -697,7 +793,7 @@ __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
                 if (reload & (1 << h)) {
                     const int f = s_frame[h];
                     const int row = f < 0 ? 0 : p.rows ? p.rows[f] : f;
-                    load_lane(c, fr, f >= 0 ? p.llr + (size_t)row * p.llr_stride : nullptr, h);
+                    load_lane<PO>(c, fr, f >= 0 ? p.llr + (size_t)row * p.llr_stride : nullptr, h);
                     fresh |= 0xFFFFu << (16 * h);
                 }
             if (t == 0)
@@ -706,7 +802,7 @@ __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
         }
         if (s_frame[0] < 0 && s_frame[1] < 0)
             break;
-        const int fail = syndrome_pair(c, fr, &s_flag, s_row);
+        const int fail = syndrome_pair<PO>(c, fr, &s_flag, s_row);
         /* lanes whose frame is done: results out, refill */
         int done = 0;
         for (int h = 0; h < 2; h++) {
@@ -732,9 +828,10 @@ __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
         if (done)
             continue; /* reload, then check the new frames first */
         if (lT)
-            iterate_pair<A, B, GDM, LS, true>(c, fr, msg, fresh, learn_row(s_iter[0], lT), learn_row(s_iter[1], lT));
+            iterate_pair<A, B, GDM, LS, true, PO>(c, fr, msg, fresh, learn_row(s_iter[0], lT),
+                                                  learn_row(s_iter[1], lT));
         else
-            iterate_pair<A, B, GDM, LS, false>(c, fr, msg, fresh, -1, -1);
+            iterate_pair<A, B, GDM, LS, false, PO>(c, fr, msg, fresh, -1, -1);
         fresh = 0;
         if (t == 0) {
             s_iter[0]++;
@@ -744,12 +841,7 @@ __global__ void __launch_bounds__(384, 1) k_decode_pair(DecodeParams p)
     }
 }
 
-size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q)
-{
-    auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
-    return a16(2 * (size_t)N) + a16(sizeof(int2) * nent) + a16(sizeof(uint16_t) * (q + 1)) +
-           a16(sizeof(uint32_t) * nsteps);
-}
+static size_t a16h(size_t v) { return (v + 15) & ~(size_t)15; }
 
 
 /* Pair kernels by information-link counts (A, B): every pair of the DVB-S2,
@@ -758,15 +850,19 @@ size_t decode_pair_smem_bytes(int N, int nent, int nsteps, int q)
  * late slots the kernel carries (two cover most levelled codes; normal 4/5
  * and 9/10 need four, short 5/6 five, short 8/9 six). */
 struct PairKernel {
-    int a, b, gdm, ls, threads;
+    int a, b, gdm, ls, po, threads;
     const void* fn;
 };
 
-#define DRXG_PKL(a, b, ls) { a, b, 0, ls, 384, (const void*)k_decode_pair<a, b, 0, ls> }
+#define DRXG_PKL(a, b, ls) { a, b, 0, ls, 0, 384, (const void*)k_decode_pair<a, b, 0, ls, false> }
 #define DRXG_PK(a, b) DRXG_PKL(a, b, 2)
 #define DRXG_PK3(a, b) DRXG_PKL(a, b, 3)
-#define DRXG_PGL(d, ls) { 0, 0, d, ls, 384, (const void*)k_decode_pair<1, 1, d, ls> }
+#define DRXG_PGL(d, ls) { 0, 0, d, ls, 0, 384, (const void*)k_decode_pair<1, 1, d, ls, false> }
 #define DRXG_PG(d) DRXG_PGL(d, 3)
+/* parity-out twins (two CTAs per SM) of the kernels that fit 80 registers */
+#define DRXG_QKL(a, b, ls) { a, b, 0, ls, 1, 384, (const void*)k_decode_pair<a, b, 0, ls, true> }
+#define DRXG_QK(a, b) DRXG_QKL(a, b, 2)
+#define DRXG_QG(d) { 0, 0, d, 3, 1, 384, (const void*)k_decode_pair<1, 1, d, 3, true> }
 static const PairKernel kPairKernels[] = {
     DRXG_PK(1, 2), DRXG_PK(2, 2), DRXG_PK(2, 3), DRXG_PK(3, 3), DRXG_PK(4, 4), DRXG_PK(5, 5),
     DRXG_PK(5, 6), DRXG_PK(6, 7), DRXG_PK(7, 7), DRXG_PK(7, 8), DRXG_PK(8, 8), DRXG_PK(8, 9),
@@ -776,22 +872,55 @@ static const PairKernel kPairKernels[] = {
     DRXG_PK(14, 15), DRXG_PKL(16, 16, 4), DRXG_PK(17, 18), DRXG_PK3(20, 20), DRXG_PKL(25, 25, 6), DRXG_PK(27, 28),
     DRXG_PKL(28, 28, 4),
     DRXG_PG(7), DRXG_PG(11), DRXG_PG(14), DRXG_PGL(22, 5), DRXG_PGL(32, 6),
+    DRXG_QK(1, 2), DRXG_QK(2, 2), DRXG_QK(2, 3), DRXG_QK(3, 3), DRXG_QK(4, 4), DRXG_QK(5, 5),
+    DRXG_QK(5, 6), DRXG_QK(6, 7), DRXG_QK(7, 7), DRXG_QK(7, 8), DRXG_QK(8, 8), DRXG_QK(8, 9),
+    DRXG_QK(9, 9), DRXG_QK(9, 10), DRXG_QK(11, 11), DRXG_QK(11, 12), DRXG_QK(12, 12), DRXG_QKL(9, 9, 3),
+    DRXG_QG(7), DRXG_QG(11), DRXG_QG(14),
 };
 #undef DRXG_PKL
 #undef DRXG_PK
 #undef DRXG_PK3
 #undef DRXG_PGL
 #undef DRXG_PG
+#undef DRXG_QKL
+#undef DRXG_QK
+#undef DRXG_QG
 constexpr int kNumPairKernels = (int)(sizeof(kPairKernels) / sizeof(kPairKernels[0]));
 
-/* message slab of one CTA: one record per check, 8 or 16 bytes */
+/* Dynamic shared memory of a pair kernel for a code: the posterior words
+ * (every bit, or the information bits of a parity-out kernel and the last
+ * parity layer), the link table, layer offsets and level steps */
+size_t decode_pair_smem_bytes(int N, int K, int nent, int nsteps, int q, int kid)
+{
+    const bool po = kid >= 0 && kid < kNumPairKernels && kPairKernels[kid].po;
+    return a16h(2 * (size_t)(po ? K : N)) + (po ? a16h(2 * (size_t)kQCp) : 0) + a16h(sizeof(int2) * nent) +
+           a16h(sizeof(uint16_t) * (q + 1)) + a16h(sizeof(uint32_t) * nsteps);
+}
+
+/* message slab of one CTA: one record per check, 8 or 16 bytes; a
+ * parity-out kernel keeps the words of parity layers 0 .. q - 2 after them */
 size_t decode_pair_msg_bytes(int R, int kid)
 {
     if (kid < 0 || kid >= kNumPairKernels)
         return 0;
     const PairKernel& k = kPairKernels[kid];
     const int dm = k.gdm > 0 ? k.gdm : k.b + 2;
-    return (size_t)R * (dm > 16 ? sizeof(uint4) : sizeof(uint2));
+    const size_t rec = a16h((size_t)R * (dm > 16 ? sizeof(uint4) : sizeof(uint2)));
+    return rec + (k.po ? a16h(sizeof(uint16_t) * (size_t)(R - kQCp)) : 0);
+}
+
+/* the parity-out twin of a kernel, -1 if it has none */
+int pair_kernel_po_twin(int kid)
+{
+    if (kid < 0 || kid >= kNumPairKernels || kPairKernels[kid].po)
+        return -1;
+    const PairKernel& k = kPairKernels[kid];
+    for (int t = 0; t < kNumPairKernels; t++) {
+        const PairKernel& u = kPairKernels[t];
+        if (u.po && u.a == k.a && u.b == k.b && u.gdm == k.gdm && u.ls == k.ls)
+            return t;
+    }
+    return -1;
 }
 
 int pair_kernel_id(const Code& c)
@@ -819,11 +948,11 @@ int pair_kernel_id(const Code& c)
     }
     if (!other)
         for (int k = 0; k < kNumPairKernels; k++)
-            if (kPairKernels[k].gdm == 0 && kPairKernels[k].a == lo && kPairKernels[k].b == hi &&
-                kPairKernels[k].ls >= ls)
+            if (!kPairKernels[k].po && kPairKernels[k].gdm == 0 && kPairKernels[k].a == lo &&
+                kPairKernels[k].b == hi && kPairKernels[k].ls >= ls)
                 return k;
     for (int k = 0; k < kNumPairKernels; k++)
-        if (kPairKernels[k].gdm >= c.deg_max && kPairKernels[k].ls >= ls)
+        if (!kPairKernels[k].po && kPairKernels[k].gdm >= c.deg_max && kPairKernels[k].ls >= ls)
             return k;
     return -1;
 }

@@ -597,15 +597,20 @@ drx_ldpc* drx_ldpc_new(const drx_fec_params* p, const char* rate)
         };
         d->pair_smem = smem_of(d->pair_kid);
         d->pair_ctas_per_sm = decode_pair_ctas_per_sm(d->pair_kid, d->pair_smem);
-        /* the parity-out twin when it makes more CTAs resident */
-        const int po = pair_kernel_po_twin(d->pair_kid);
-        if (po >= 0) {
-            const size_t sm = smem_of(po);
-            const int n = decode_pair_ctas_per_sm(po, sm);
+        /* a two-CTA twin when it makes more CTAs resident: all posteriors in
+         * shared memory if they leave room, else the parity-out one */
+        const int base = d->pair_kid;
+        for (int pm = 1; pm <= 2; pm++) {
+            const int tw = pair_kernel_twin(base, pm);
+            if (tw < 0)
+                continue;
+            const size_t sm = smem_of(tw);
+            const int n = decode_pair_ctas_per_sm(tw, sm);
             if (n > d->pair_ctas_per_sm) {
-                d->pair_kid = po;
+                d->pair_kid = tw;
                 d->pair_smem = sm;
                 d->pair_ctas_per_sm = n;
+                break;
             }
         }
     }

@@ -143,10 +143,10 @@ namespace drxg {
  * instantiation for a code (-1: not run by the frame-pair kernel). */
 struct Code;
 int pair_kernel_id(const Code& c);
-/* The parity-out twin of kernel kid (parity posteriors in the CTA's global
- * slab and registers, about half the shared memory, two CTAs per SM), -1 if
- * it has none */
-int pair_kernel_po_twin(int kid);
+/* The twin of kernel kid compiled for two CTAs per SM: pm 1 keeps every
+ * posterior in shared memory, pm 2 keeps the parity posteriors in the CTA's
+ * global slab and in registers (about half the shared memory); -1 if none */
+int pair_kernel_twin(int kid, int pm);
 size_t decode_pair_smem_bytes(int N, int K, int nent, int nsteps, int q, int kid);
 size_t decode_pair_msg_bytes(int R, int kid);
 int decode_pair_ctas_per_sm(int kid, size_t smem);

@@ -603,14 +603,17 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, 
     const bool active = t < kQCp;
     Rec rn{};
     unsigned long long mn = 0;
-    /* PO: the word of parity bit (i, j) for layer i (loaded a layer ahead),
-     * and of (i - 1, j), which the previous layer of this thread wrote */
-    uint32_t pnext = 0, carry = 0;
+    /* PO: the words of parity bits (i, j) and (i + 1, j) for layers i and
+     * i + 1 (loaded two layers ahead), and of (i - 1, j), which the previous
+     * layer of this thread wrote */
+    uint32_t pnext = 0, pnext2 = 0, carry = 0;
     if (active) {
         rn = __ldcg(msg + j);
         mn = __ldg(c.lmeta + j);
         if (PO && c.q > 1)
             pnext = fr.gpar[j];
+        if (PO && c.q > 2)
+            pnext2 = fr.gpar[kQCp + j];
     }
     for (int i = 0; i < c.q; i++) {
         const Rec rec = rn;
@@ -622,8 +625,9 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, 
         }
         if (PO && active) {
             r0 = i + 1 < c.q ? pnext : fr.wrap[j];
-            if (i + 2 < c.q)
-                pnext = fr.gpar[kQCp * (i + 1) + j];
+            pnext = pnext2;
+            if (i + 3 < c.q)
+                pnext2 = fr.gpar[kQCp * (i + 2) + j];
             r1 = i ? carry : (j ? fr.wrap[j - 1] : 0u);
         }
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
@@ -703,11 +707,13 @@ __device__ int pair_team_vote(unsigned* slot, int M, bool fail, int* err)
     return r;
 }
 
-/* PO: parity posteriors out of shared memory (two CTAs per SM for normal
- * frames up to rate 4/5); the kernel is then compiled for two resident CTAs */
-template <int A, int B, int GDM, int LS, bool PO>
-__global__ void __launch_bounds__(384, PO ? 2 : 1) k_decode_pair(DecodeParams p)
+/* PM: 0 one resident CTA per SM; 1 two (80 registers), for codes whose
+ * posteriors leave room for two (short frames); 2 two, with the parity
+ * posteriors out of shared memory (PO: normal frames up to rate 3/4) */
+template <int A, int B, int GDM, int LS, int PM>
+__global__ void __launch_bounds__(384, PM ? 2 : 1) k_decode_pair(DecodeParams p)
 {
+    constexpr bool PO = PM == 2;
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_frame[2], s_iter[2], s_flag, s_reload, s_row[2];
     const DevCode c = *p.code;
@@ -850,19 +856,21 @@ static size_t a16h(size_t v) { return (v + 15) & ~(size_t)15; }
  * late slots the kernel carries (two cover most levelled codes; normal 4/5
  * and 9/10 need four, short 5/6 five, short 8/9 six). */
 struct PairKernel {
-    int a, b, gdm, ls, po, threads;
+    int a, b, gdm, ls, pm, threads;
     const void* fn;
 };
 
-#define DRXG_PKL(a, b, ls) { a, b, 0, ls, 0, 384, (const void*)k_decode_pair<a, b, 0, ls, false> }
+#define DRXG_PKL(a, b, ls) { a, b, 0, ls, 0, 384, (const void*)k_decode_pair<a, b, 0, ls, 0> }
 #define DRXG_PK(a, b) DRXG_PKL(a, b, 2)
 #define DRXG_PK3(a, b) DRXG_PKL(a, b, 3)
-#define DRXG_PGL(d, ls) { 0, 0, d, ls, 0, 384, (const void*)k_decode_pair<1, 1, d, ls, false> }
+#define DRXG_PGL(d, ls) { 0, 0, d, ls, 0, 384, (const void*)k_decode_pair<1, 1, d, ls, 0> }
 #define DRXG_PG(d) DRXG_PGL(d, 3)
-/* parity-out twins (two CTAs per SM) of the kernels that fit 80 registers */
-#define DRXG_QKL(a, b, ls) { a, b, 0, ls, 1, 384, (const void*)k_decode_pair<a, b, 0, ls, true> }
+/* two-CTA twins (modes 1 and 2) of the kernels that fit 80 registers */
+#define DRXG_QKL(a, b, ls) { a, b, 0, ls, 1, 384, (const void*)k_decode_pair<a, b, 0, ls, 1> }, \
+                           { a, b, 0, ls, 2, 384, (const void*)k_decode_pair<a, b, 0, ls, 2> }
 #define DRXG_QK(a, b) DRXG_QKL(a, b, 2)
-#define DRXG_QG(d) { 0, 0, d, 3, 1, 384, (const void*)k_decode_pair<1, 1, d, 3, true> }
+#define DRXG_QG(d) { 0, 0, d, 3, 1, 384, (const void*)k_decode_pair<1, 1, d, 3, 1> }, \
+                   { 0, 0, d, 3, 2, 384, (const void*)k_decode_pair<1, 1, d, 3, 2> }
 static const PairKernel kPairKernels[] = {
     DRXG_PK(1, 2), DRXG_PK(2, 2), DRXG_PK(2, 3), DRXG_PK(3, 3), DRXG_PK(4, 4), DRXG_PK(5, 5),
     DRXG_PK(5, 6), DRXG_PK(6, 7), DRXG_PK(7, 7), DRXG_PK(7, 8), DRXG_PK(8, 8), DRXG_PK(8, 9),
@@ -892,7 +900,7 @@ constexpr int kNumPairKernels = (int)(sizeof(kPairKernels) / sizeof(kPairKernels
  * parity layer), the link table, layer offsets and level steps */
 size_t decode_pair_smem_bytes(int N, int K, int nent, int nsteps, int q, int kid)
 {
-    const bool po = kid >= 0 && kid < kNumPairKernels && kPairKernels[kid].po;
+    const bool po = kid >= 0 && kid < kNumPairKernels && kPairKernels[kid].pm == 2;
     return a16h(2 * (size_t)(po ? K : N)) + (po ? a16h(2 * (size_t)kQCp) : 0) + a16h(sizeof(int2) * nent) +
            a16h(sizeof(uint16_t) * (q + 1)) + a16h(sizeof(uint32_t) * nsteps);
 }
@@ -906,18 +914,18 @@ size_t decode_pair_msg_bytes(int R, int kid)
     const PairKernel& k = kPairKernels[kid];
     const int dm = k.gdm > 0 ? k.gdm : k.b + 2;
     const size_t rec = a16h((size_t)R * (dm > 16 ? sizeof(uint4) : sizeof(uint2)));
-    return rec + (k.po ? a16h(sizeof(uint16_t) * (size_t)(R - kQCp)) : 0);
+    return rec + (k.pm == 2 ? a16h(sizeof(uint16_t) * (size_t)(R - kQCp)) : 0);
 }
 
-/* the parity-out twin of a kernel, -1 if it has none */
-int pair_kernel_po_twin(int kid)
+/* the twin of a mode-0 kernel in mode pm (1 or 2), -1 if it has none */
+int pair_kernel_twin(int kid, int pm)
 {
-    if (kid < 0 || kid >= kNumPairKernels || kPairKernels[kid].po)
+    if (kid < 0 || kid >= kNumPairKernels || kPairKernels[kid].pm != 0)
         return -1;
     const PairKernel& k = kPairKernels[kid];
     for (int t = 0; t < kNumPairKernels; t++) {
         const PairKernel& u = kPairKernels[t];
-        if (u.po && u.a == k.a && u.b == k.b && u.gdm == k.gdm && u.ls == k.ls)
+        if (u.pm == pm && u.a == k.a && u.b == k.b && u.gdm == k.gdm && u.ls == k.ls)
             return t;
     }
     return -1;
@@ -948,11 +956,11 @@ int pair_kernel_id(const Code& c)
     }
     if (!other)
         for (int k = 0; k < kNumPairKernels; k++)
-            if (!kPairKernels[k].po && kPairKernels[k].gdm == 0 && kPairKernels[k].a == lo &&
+            if (kPairKernels[k].pm == 0 && kPairKernels[k].gdm == 0 && kPairKernels[k].a == lo &&
                 kPairKernels[k].b == hi && kPairKernels[k].ls >= ls)
                 return k;
     for (int k = 0; k < kNumPairKernels; k++)
-        if (!kPairKernels[k].po && kPairKernels[k].gdm >= c.deg_max && kPairKernels[k].ls >= ls)
+        if (kPairKernels[k].pm == 0 && kPairKernels[k].gdm >= c.deg_max && kPairKernels[k].ls >= ls)
             return k;
     return -1;
 }

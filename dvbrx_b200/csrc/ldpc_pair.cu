@@ -709,7 +709,7 @@ __device__ int pair_team_vote(unsigned* slot, int M, bool fail, int* err)
 
 /* PM: 0 one resident CTA per SM; 1 two (80 registers), for codes whose
  * posteriors leave room for two (short frames); 2 two, with the parity
- * posteriors out of shared memory (PO: normal frames up to rate 3/4) */
+ * posteriors out of shared memory (PO: normal frames up to rate 4/5) */
 template <int A, int B, int GDM, int LS, int PM>
 __global__ void __launch_bounds__(384, PM ? 2 : 1) k_decode_pair(DecodeParams p)
 {
@@ -884,6 +884,8 @@ static const PairKernel kPairKernels[] = {
     DRXG_QK(5, 6), DRXG_QK(6, 7), DRXG_QK(7, 7), DRXG_QK(7, 8), DRXG_QK(8, 8), DRXG_QK(8, 9),
     DRXG_QK(9, 9), DRXG_QK(9, 10), DRXG_QK(11, 11), DRXG_QK(11, 12), DRXG_QK(12, 12), DRXG_QKL(9, 9, 3),
     DRXG_QG(7), DRXG_QG(11), DRXG_QG(14),
+    /* normal 4/5 (16-byte records): parity out only, its posteriors leave no room otherwise */
+    { 16, 16, 0, 4, 2, 384, (const void*)k_decode_pair<16, 16, 0, 4, 2> },
 };
 #undef DRXG_PKL
 #undef DRXG_PK

@@ -886,6 +886,9 @@ static const PairKernel kPairKernels[] = {
     DRXG_QG(7), DRXG_QG(11), DRXG_QG(14),
     /* normal 4/5 (16-byte records): parity out only, its posteriors leave no room otherwise */
     { 16, 16, 0, 4, 2, 384, (const void*)k_decode_pair<16, 16, 0, 4, 2> },
+    /* short 5/6 and 8/9: two CTAs with every posterior in shared memory */
+    { 0, 0, 22, 5, 1, 384, (const void*)k_decode_pair<1, 1, 22, 5, 1> },
+    { 25, 25, 0, 6, 1, 384, (const void*)k_decode_pair<25, 25, 0, 6, 1> },
 };
 #undef DRXG_PKL
 #undef DRXG_PK

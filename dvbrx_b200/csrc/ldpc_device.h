@@ -139,8 +139,10 @@ cudaError_t launch_decode(const DecodeParams& p, int dclass, size_t smem, int gr
 namespace drxg {
 
 /* Frame-pair variant (ldpc_pair.cu): two frames per CTA in 16x2 SIMD, codes
- * up to check degree 32; per-frame stopping only.  pair_kernel_id picks the
- * instantiation for a code (-1: not run by the frame-pair kernel). */
+ * up to check degree 32; per-frame stopping, or group stopping on teams of
+ * co-resident CTAs.  pair_kernel_id picks the one-CTA-per-SM instantiation
+ * for a code (-1: not run by the frame-pair kernel); pair_kernel_twin gives
+ * its two-CTA forms. */
 struct Code;
 int pair_kernel_id(const Code& c);
 /* The twin of kernel kid compiled for two CTAs per SM: pm 1 keeps every

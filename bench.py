@@ -25,7 +25,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -54,10 +53,15 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=7)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned decoder's line items")
     ap.add_argument("--no-bch", action="store_true", help="skip the BCH line item")
+    ap.add_argument("--no-group", action="store_true", help="skip the 64-frame group-stopping line item")
     ap.add_argument("--mix-frames", type=int, default=16384,
                     help="frames of the mixed-MODCOD batch (0: skip that line item)")
     ap.add_argument("--variant", default="auto", choices=["auto", "frame"],
                     help="decoder kernel: automatic choice, or the one-frame kernel")
+    ap.add_argument("--per-code", action="store_true",
+                    help="print the per-code cost table (us per frame-iteration) instead of the JSON line")
+    ap.add_argument("--rates", nargs="*", default=None, help="--per-code: the rates (default: every DVB-S2 rate)")
+    ap.add_argument("--short", action="store_true", help="--per-code: short frames")
     ap.add_argument("--batches", type=int, default=len(ESN0),
                     help="Es/N0 points held on the device (small profiling cases use fewer)")
     return ap.parse_args()
@@ -160,102 +164,78 @@ def profiled_figures():
 # CPU: the reference decoder compiled from its sources (oracle/_ref)
 # ---------------------------------------------------------------------------
 
-def cpu_reference_run(llr_batches, seconds, threads):
-    """Reference production mode (rxmt.c:514-536): one thread per core, each
-    with its own handle, decoding batches of `lanes` frames with
-    drx_ldpc_decode.  Runs for about `seconds`; returns (frames/s, lanes,
-    frames, threads)."""
+def cpu_description(ref):
+    """The host CPU and the reference build that runs on it."""
     import oracle
-    lib = oracle.load_ref()
-    if lib is None:
-        raise RuntimeError("reference decoder not built (make -C oracle ref)")
-    lanes = lib.ref_ldpc_lanes()
-    counts = [0] * threads
-    stop_at = [0.0]
-    barrier = threading.Barrier(threads + 1)
-
-    def worker(w):
-        ref = oracle.RefCode(SHORT, RATE)
-        nb = len(llr_batches)
-        k = w
-        barrier.wait()
-        while time.perf_counter() < stop_at[0]:
-            batch = llr_batches[k % nb]
-            g0 = (k // nb * lanes) % max(1, batch.shape[0] - lanes + 1)
-            ref.decode_call(batch[g0:g0 + lanes], MAX_ITER)
-            counts[w] += lanes
-            k += threads
-
-    ts = [threading.Thread(target=worker, args=(w,)) for w in range(threads)]
-    for t in ts:
-        t.start()
-    t0 = time.perf_counter()
-    stop_at[0] = t0 + seconds
-    barrier.wait()
-    t0 = time.perf_counter()
-    for t in ts:
-        t.join()
-    dt = time.perf_counter() - t0
-    return sum(counts) / dt, lanes, sum(counts), threads
+    c = oracle.cpu_info()
+    return {"cpu_model": c["model"], "physical_cores": c["physical_cores"], "logical_cpus": c["logical_cpus"],
+            "ref_build": "libref_%s.so" % ref.flavour, "march": oracle.flavour_march(ref.flavour),
+            "march_note": "compiled for this host's CPU (what -march=native gives here)"
+                          if oracle.native_arch() == ref.flavour else
+                          "portable ISA level (no build for this CPU model)",
+            "lanes": ref.lanes}
 
 
-def host_llr_batches(frames_per_point, seed=99):
-    """Input frames for the CPU-only arm, made on the CPU (numpy channel)."""
+def cpu_reference_run(pool, seconds, threads):
+    """Reference production mode (rxmt.c:514-536): persistent worker
+    threads, each with its own handle, decoding batches of `lanes` frames
+    with drx_ldpc_decode (oracle/refbench.c, CLOCK_MONOTONIC) for about
+    `seconds`.  Returns (frames/s, frames, RefCode)."""
+    import oracle
+    ref = oracle.RefCode(SHORT, RATE)
+    ref.bench(pool, MAX_ITER, threads, seconds=min(1.0, seconds))  # warm-up: pages, caches, clocks
+    step_s, calls = ref.bench(pool, MAX_ITER, threads, seconds=seconds)
+    return calls * ref.lanes / step_s[0], calls * ref.lanes, ref
+
+
+def host_llr_pool(frames_per_point, seed=99):
+    """Input frames of the CPU-only arm, made on the CPU (numpy channel):
+    the sweep's seven Es/N0 points, one after the other."""
     from oracle import OrcCode, datagen
     code = OrcCode(SHORT, RATE)
     out = []
     for k, es in enumerate(ESN0):
         d = datagen.make_frames(SHORT, RATE, frames_per_point, es, CONST, seed=seed + k, code=code)
         out.append(d["llr"])
-    return out
+    return np.concatenate(out)
 
 
 def run_reference(args):
+    """The reference's own CPU decoder on this host's cores: every step
+    decodes as many frames as one GPU step (args.frames) in calls of `lanes`
+    frames, shared by persistent worker threads (one handle each, one per
+    logical CPU), steps separated by barriers; only rank 0 runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
     import oracle
     lib = oracle.load_ref()
-    if lib is None:
+    if lib is None or not hasattr(lib, "refx_bench"):
         print(json.dumps({"impl": "reference", "unavailable": "reference decoder not built (oracle/_ref missing)"}))
         return
-    lanes = lib.ref_ldpc_lanes()
-    batches = host_llr_batches(lanes)
-    # one step: every thread decodes one batch of `lanes` frames
-    import oracle as _o
-    refs = [_o.RefCode(SHORT, RATE) for _ in range(threads)]
-
-    def step(k):
-        def w(i):
-            refs[i].decode_call(batches[(k + i) % len(batches)], MAX_ITER)
-        ts = [threading.Thread(target=w, args=(i,)) for i in range(threads)]
-        for t in ts:
-            t.start()
-        for t in ts:
-            t.join()
-
-    for k in range(args.warmup):
-        step(k)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        step(args.warmup + k)
-    dt = time.perf_counter() - t0
-    frames = args.steps * threads * lanes
+    threads = oracle.host_threads()
+    ref = oracle.RefCode(SHORT, RATE)
+    lanes = ref.lanes
+    pool = host_llr_pool(128)
+    calls = max(1, args.frames // lanes)
+    step_s, ncalls = ref.bench(pool, MAX_ITER, threads, steps=args.warmup + args.steps, calls_per_step=calls)
+    dt = float(step_s[args.warmup:].sum())
+    frames = args.steps * calls * lanes
     gbps = frames * 38880 / dt / 1e9
+    cpu = {"value": gbps, "unit": UNIT, "cores": threads, "kind": "reference",
+           "sample": "%d steps x %d drx_ldpc_decode calls of %d frames (the sweep's 7 Es/N0 points, 128 "
+                     "frames each), %d persistent threads" % (args.steps, calls, lanes, threads)}
+    cpu.update(cpu_description(ref))
     line = {
         "metric": METRIC, "value": gbps, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
         "impl": "reference",
-        "config": dict(workload_config(lanes * threads, 1),
+        "config": dict(workload_config(calls * lanes, 1),
                        stopping="per batch of %d frames (reference drx_ldpc_decode semantics)" % lanes,
-                       frames_per_step=lanes * threads, l2="n/a (host CPU)",
-                       parallelism="one thread and one decoder handle per host core"),
-        "cpu_baseline": {"value": gbps, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "lanes": lanes,
-                         "sample": "%d steps x %d threads x one %d-frame drx_ldpc_decode call" % (
-                             args.steps, threads, lanes)},
+                       frames_per_step=calls * lanes, l2="n/a (host CPU)",
+                       parallelism="persistent worker threads, one decoder handle each, one per logical CPU"),
+        "cpu_baseline": cpu,
         "e2e": {"value": gbps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -578,6 +558,34 @@ def run_b200(args):
         "sm_mhz_median": sm_mhz,
     }
 
+    # the same batches with the reference's batch semantics: groups of 64
+    # frames (drx_ldpc_decode on 64 lanes) iterate until all their frames pass
+    group64 = None
+    if not args.no_group:
+        g_it = [torch.empty(F, dtype=torch.int32, device="cuda") for _ in range(args.steps)]
+        g_ok = [torch.empty(F, dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
+        for k in range(min(args.warmup, 3)):
+            dec.decode_device(llr[k % len(llr)], MAX_ITER, out=outs[0], iters=g_it[0], ok=g_ok[0], stop=64)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            gev[k][0].record(stream)
+            dec.decode_device(llr[(args.warmup + k) % len(llr)], MAX_ITER, out=outs[k], iters=g_it[k], ok=g_ok[k],
+                              stop=64)
+            gev[k][1].record(stream)
+        torch.cuda.synchronize()
+        g_ms = max_over_ranks(gev[0][0].elapsed_time(gev[-1][1]), world, "cuda")
+        g_iters = torch.stack(g_it).to(torch.int64)
+        group64 = {"value": aggregate_gbps(world, frames_rank, kldpc, g_ms), "unit": UNIT,
+                   "ms_per_step": g_ms / args.steps,
+                   "stopping": "groups of 64 consecutive frames stop together (the reference's "
+                               "drx_ldpc_decode batch semantics on 64 lanes)",
+                   "avg_iterations": float(g_iters.float().mean()),
+                   "frame_iterations_vs_per_frame": float(g_iters.sum()) / max(1, iters_sum),
+                   "launch": "one cooperative launch per step, teams of 32 co-resident CTAs per group"}
+
     # the learned decoder (committed 12-iteration table, int8) with the plain
     # decoder as fallback, on the same batches and steps
     learned = None
@@ -657,15 +665,17 @@ def run_b200(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            host_b = [l[: 4 * 64].cpu().numpy() for l in llr]
-            threads = os.cpu_count() or 1
-            fps, lanes, nf, thr = cpu_reference_run(host_b, args.cpu_seconds, threads)
-            fps1, _, _, _ = cpu_reference_run(host_b, min(3.0, args.cpu_seconds), 1)
-            cpu = {"value": fps * kldpc / 1e9, "unit": UNIT, "cores": thr, "kind": "reference",
-                   "lanes": lanes, "value_1core": fps1 * kldpc / 1e9,
-                   "sample": "%d frames in %.0f s: batches of %d frames (drx_ldpc_decode), one "
-                             "thread and handle per core, the same int8 LLRs as the GPU, all 7 Es/N0 points"
-                             % (nf, args.cpu_seconds, lanes)}
+            import oracle
+            pool = np.concatenate([l[:128].cpu().numpy() for l in llr])
+            threads = oracle.host_threads()
+            fps, nf, ref = cpu_reference_run(pool, args.cpu_seconds, threads)
+            fps1, _, _ = cpu_reference_run(pool, min(3.0, args.cpu_seconds), 1)
+            cpu = {"value": fps * kldpc / 1e9, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "value_1core": fps1 * kldpc / 1e9,
+                   "sample": "%d frames in %.0f s: drx_ldpc_decode calls of %d frames by %d persistent "
+                             "threads (one handle each), the same int8 LLRs as the GPU (128 frames of each "
+                             "Es/N0 point)" % (nf, args.cpu_seconds, ref.lanes, threads)}
+            cpu.update(cpu_description(ref))
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "failed: %s" % e}
 
@@ -677,7 +687,8 @@ def run_b200(args):
             "config": workload_config(F, world),
             "decoder": "plain layered offset min-sum (bit-exact to the reference)",
             "quality": {"fer": fer, "avg_iterations": iters_sum / frames_rank},
-            "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "learned": learned,
+            "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "group64": group64,
+            "learned": learned,
             "mixed_modcod": mix_res, "mixed_modcod_learned": mix_learned, "bch": bch, "demapper": demap,
             "gpu_launches": args.steps,
         }
@@ -687,10 +698,65 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+NORMAL_RATES = ["1_4", "1_3", "2_5", "1_2", "3_5", "2_3", "3_4", "4_5", "5_6", "8_9", "9_10"]
+
+
+def frame_iteration_us(dec, variant, n, seed=7):
+    """Microseconds of the whole GPU per frame-iteration of one kernel on one
+    code: n frames generated far below the code's threshold (no frame
+    converges, every frame runs its iterations); (t(30) - t(10)) / 20 / n
+    from CUDA events, best of five."""
+    import torch
+
+    import dvbrx_b200 as D
+
+    dec.set_variant(variant)
+    llr, _, _ = dec.generate(n, -6.0, seed=seed)
+    t = {}
+    for it in (10, 30):
+        best = float("inf")
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            _, _, ok = dec.decode_device(llr, it)
+            b.record()
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        t[it] = best
+    assert int(ok.sum()) == 0, "a frame converged: the case must stay below threshold"
+    dec.set_variant(D.VARIANT_AUTO)
+    return (t[30] - t[10]) / 20 * 1e3 / n
+
+
+def run_per_code(args):
+    """--per-code: decoder cost per DVB-S2 code (frame-pair kernel against
+    the one-frame kernel), several full waves of frames per code (6 per SM
+    for normal frames, 24 for short ones: every CTA of either kernel busy).
+    Prints a table, not the JSON line."""
+    import torch
+
+    import dvbrx_b200 as D
+
+    short = int(args.short)
+    n = (24 if short else 6) * torch.cuda.get_device_properties(0).multi_processor_count
+    print("%-6s %-6s %12s %12s %8s" % ("frame", "rate", "pair us", "frame us", "ratio"))
+    for rate in args.rates or NORMAL_RATES:
+        if short and rate == "9_10":
+            continue
+        dec = D.Ldpc(D.fec_lookup(short, rate), rate)
+        pair = frame_iteration_us(dec, D.VARIANT_PAIR, n)
+        one = frame_iteration_us(dec, D.VARIANT_FRAME, n)
+        print("%-6s %-6s %12.3f %12.3f %8.2f" % ("short" if short else "normal", rate, pair, one, one / pair))
+        dec.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.per_code:
+        run_per_code(args)
     else:
         run_b200(args)
 

@@ -979,6 +979,17 @@ const DevCode* handle_code(const drx_ldpc* d, int* R, int* dclass, int* N, int* 
     return d->dcode;
 }
 
+/* The frame-pair kernel of a handle's per-frame calls (-1: the one-frame
+ * kernel), its dynamic shared memory and resident CTAs. */
+int handle_pair(const drx_ldpc* d, size_t* smem, int* capacity)
+{
+    if (!use_pair(d))
+        return -1;
+    *smem = d->pair_smem;
+    *capacity = d->pair_ctas_per_sm * d->sms;
+    return d->pair_kid;
+}
+
 void handle_set_error(const char* msg) { set_err(msg); }
 
 }  // namespace drxg

@@ -16,17 +16,29 @@
  * The scratch is g_scratch below: 16 MiB of device memory that every GPU
  * which loads the library holds until the process exits.  Bytes [0, 256)
  * hold the frame counter and an error word, cleared by every call; the rest
- * holds one message slab per CTA (R words of 4 bytes, 8 above check degree
- * 16), so a call runs at most (16 MiB - 256) / slab CTAs: 161 for normal 3/5,
- * 466 for short 1/2.  Every call shares the array and leaves its contents
- * behind; calls whose kernels overlap on the GPU (concurrent streams, or
- * several host threads) race on it and must be serialised by the caller.
+ * holds one message slab per CTA.  The call runs the kernel the regular
+ * entry point runs for the handle: the frame-pair kernel (two frames per
+ * CTA) where the handle uses it, its slab holding an 8- or 16-byte record
+ * per check and, for the parity-out kernels of normal frames up to rate 4/5,
+ * two bytes per parity bit; otherwise the one-frame kernel (R words of 4
+ * bytes, 8 above check degree 16).  A call therefore runs at most
+ * (16 MiB - 256) / slab CTAs: 64 frame-pair CTAs (128 frames at a time,
+ * one CTA on each of 64 SMs) for normal 3/5, against the 296 CTAs (two on
+ * every SM) of the regular call, so that large batches decode more slowly
+ * than through drx_ldpc_decode_device; 233 frame-pair CTAs (of 296) for
+ * short 1/2.
+ * Every call shares the array and leaves its contents behind; calls whose
+ * kernels overlap on the GPU (concurrent streams, or several host threads)
+ * race on it and must be serialised by the caller.
  *
  * Host code cannot use the name g_scratch as a device address (in host code
  * it names a host-side stand-in): the device address comes from
  * cudaGetSymbolAddress, looked up once per device, with that device
- * current, on the first call made on it.  That first call therefore does
- * the set-up and must come before any stream capture.
+ * current.  The first call made on a device does that set-up, which can
+ * load this file's module and so allocate and synchronise: make one call
+ * with nframes = 0 per device at initialisation, before any stream capture
+ * and before the real-time path starts (it does the set-up and decodes
+ * nothing).
  */
 #include <cuda_runtime.h>
 
@@ -73,6 +85,7 @@ void* scratch_address(int dev)
 namespace drxg {
 const DevCode* handle_code(const drx_ldpc* d, int* R, int* dclass, int* N, int* nbytes, int* capacity,
                            size_t* smem, cudaStream_t* stream);
+int handle_pair(const drx_ldpc* d, size_t* smem, int* capacity);
 void handle_set_error(const char* msg);
 }  // namespace drxg
 
@@ -85,6 +98,17 @@ extern "C" int drx_ldpc_decode_device_noalloc(drx_ldpc* d, const int8_t* llr, si
         handle_set_error("NULL argument");
         return -1;
     }
+    /* the per-device set-up first: a call with no frames does only that */
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        handle_set_error("drx_ldpc_decode_device_noalloc: no usable current device");
+        return -1;
+    }
+    unsigned char* base = (unsigned char*)scratch_address(dev);
+    if (!base) {
+        handle_set_error(g_noalloc_err.c_str());
+        return -1;
+    }
     if (nframes <= 0)
         return 0;
     int R = 0, dclass = 0, N = 0, nbytes = 0, capacity = 0;
@@ -95,22 +119,16 @@ extern "C" int drx_ldpc_decode_device_noalloc(drx_ldpc* d, const int8_t* llr, si
         handle_set_error("row stride below the frame size");
         return -1;
     }
-    const size_t slab = decode_msg_bytes(R, dclass);
+    /* the frame-pair kernel where the regular entry point runs it */
+    size_t pair_smem = 0;
+    int pair_capacity = 0;
+    const int kid = handle_pair(d, &pair_smem, &pair_capacity);
+    const size_t slab = kid >= 0 ? decode_pair_msg_bytes(R, kid) : decode_msg_bytes(R, dclass);
     const size_t fit = (kScratchBytes - kHeader) / slab;
     if (fit < 1) {
         handle_set_error(("drx_ldpc_decode_device_noalloc: one CTA needs " + std::to_string(slab) +
                           " bytes of scratch, more than the " + std::to_string(kScratchBytes - kHeader) +
                           " the static array holds").c_str());
-        return -1;
-    }
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-        handle_set_error("drx_ldpc_decode_device_noalloc: no usable current device");
-        return -1;
-    }
-    unsigned char* base = (unsigned char*)scratch_address(dev);
-    if (!base) {
-        handle_set_error(g_noalloc_err.c_str());
         return -1;
     }
     cudaStream_t s = stream ? (cudaStream_t)stream : own;
@@ -135,8 +153,13 @@ extern "C" int drx_ldpc_decode_device_noalloc(drx_ldpc* d, const int8_t* llr, si
     p.err = (int*)(base + 4);
     p.msg = base + kHeader;
     p.msg_stride = slab;
-    const int grid = (int)std::min<size_t>({ (size_t)nframes, (size_t)capacity, fit });
-    e = launch_decode(p, dclass, smem, grid, s);
+    if (kid >= 0) {
+        const int grid = (int)std::min<size_t>({ (size_t)(nframes + 1) / 2, (size_t)pair_capacity, fit });
+        e = launch_decode_pair(p, kid, pair_smem, grid, s);
+    } else {
+        const int grid = (int)std::min<size_t>({ (size_t)nframes, (size_t)capacity, fit });
+        e = launch_decode(p, dclass, smem, grid, s);
+    }
     if (e != cudaSuccess) {
         handle_set_error(cudaGetErrorString(e));
         return -1;

@@ -106,13 +106,20 @@ int drx_ldpc_decode_device(drx_ldpc* d, const int8_t* llr, size_t llr_stride, ui
  * device-wide synchronisation; a program whose GPU memory belongs to
  * another allocator): the call allocates nothing.  Its scratch is a 16 MiB
  * array compiled into the library, held by every GPU that loads it until
- * exit; at most (16 MiB - 256) / (R * 4 bytes, 8 above check degree 16)
- * CTAs run (161 for normal 3/5), and a code whose message slab would not
- * fit is rejected with an error.  All calls share that array: calls whose
- * kernels overlap on the GPU race and must be serialised by the caller.
- * The first call on a device looks up the array's device address (set-up)
- * and must come before any stream capture.  The handle is made by
- * drx_ldpc_new beforehand.  Returns 0 if the work was queued. */
+ * exit.  It runs the kernel drx_ldpc_decode_device runs for the handle
+ * (the frame-pair kernel, or the one-frame kernel where the handle is
+ * pinned to it), on at most (16 MiB - 256) / slab CTAs, the slab being the
+ * kernel's message scratch per CTA: 64 frame-pair CTAs for normal 3/5
+ * (against 296 in the regular call), 233 for short 1/2; a code whose slab
+ * would not fit is rejected with an error.  Large batches therefore decode
+ * more slowly than through drx_ldpc_decode_device.  All calls share that
+ * array: calls whose kernels overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the
+ * array's device address (set-up, which can load the library's device
+ * code and allocate): make one call with nframes = 0 on every device at
+ * initialisation, before any stream capture; it decodes nothing.  The
+ * handle is made by drx_ldpc_new beforehand.  Returns 0 if the work was
+ * queued. */
 int drx_ldpc_decode_device_noalloc(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out,
                                    size_t out_stride, int32_t* iters, uint8_t* ok, int nframes,
                                    int max_iter, void* stream);

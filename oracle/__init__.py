@@ -50,13 +50,80 @@ def cpu_flags():
     return set()
 
 
+def cpu_info():
+    """The host CPU: model name, vendor family/model, logical CPUs this
+    process may use and physical cores (distinct (package, core) pairs)."""
+    model, vendor, family, mnum = "unknown", "", -1, -1
+    cores = set()
+    pkg = core = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name" and model == "unknown":
+                    model = v
+                elif k == "vendor_id" and not vendor:
+                    vendor = v
+                elif k == "cpu family" and family < 0:
+                    family = int(v)
+                elif k == "model" and mnum < 0:
+                    mnum = int(v)
+                elif k == "physical id":
+                    pkg = v
+                elif k == "core id":
+                    core = v
+                elif not k and pkg is not None:
+                    cores.add((pkg, core))
+                    pkg = core = None
+        if pkg is not None:
+            cores.add((pkg, core))
+    except OSError:
+        pass
+    try:
+        logical = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        logical = os.cpu_count() or 1
+    return {"model": model, "vendor": vendor, "family": family, "model_number": mnum,
+            "logical_cpus": logical, "physical_cores": len(cores) or None}
+
+
+def native_arch():
+    """The gcc -march name of this host's CPU among the oracle's native
+    builds (oracle/Makefile NATIVE_ARCHS), or None."""
+    c = cpu_info()
+    if c["vendor"] == "GenuineIntel" and c["family"] == 6:
+        return {143: "sapphirerapids", 207: "emeraldrapids", 173: "graniterapids",
+                174: "graniterapids"}.get(c["model_number"])
+    if c["vendor"] == "AuthenticAMD":
+        if c["family"] == 25 and (0x10 <= c["model_number"] <= 0x1F or 0xA0 <= c["model_number"] <= 0xAF):
+            return "znver4"
+        if c["family"] == 26:
+            return "znver5"
+    return None
+
+
 def best_ref_flavour():
+    """The reference build for this host: the one compiled for its CPU
+    (what -march=native gives) if present, else the widest portable one
+    its instruction set runs."""
+    arch = native_arch()
+    if arch and os.path.exists(os.path.join(REF_DIR, "libref_%s.so" % arch)):
+        return arch
     flags = cpu_flags()
     if "avx512bw" in flags and "avx512vl" in flags and "avx512dq" in flags:
         return "avx512"
     if "avx2" in flags and "fma" in flags:
         return "avx2"
     return "sse2"
+
+
+MARCH = {"avx512": "x86-64-v4", "avx2": "x86-64-v3", "sse2": "x86-64-v2"}
+
+
+def flavour_march(flavour):
+    """The -march a reference build was compiled with."""
+    return MARCH.get(flavour, flavour)
 
 
 _orc = None
@@ -119,8 +186,24 @@ def load_ref(flavour=None):
     lib.ref_demap_frame.argtypes = [vp, vp, ctypes.c_float, vp]
     lib.ref_demap_symbols.argtypes = [vp]
     lib.ref_demap_symbols.restype = ip
+    sz, dp = ctypes.c_size_t, ctypes.c_double
+    if hasattr(lib, "refx_bench"):
+        fp = ctypes.POINTER(FecParams)
+        lib.refx_decode_frames_mt.argtypes = [fp, cp, vp, sz, ip, ip, vp, sz, vp, vp, ip]
+        lib.refx_decode_frames_mt.restype = ip
+        lib.refx_decode_groups_mt.argtypes = [fp, cp, vp, sz, ip, ip, ip, vp, sz, vp, ip]
+        lib.refx_decode_groups_mt.restype = ip
+        lib.refx_bench.argtypes = [fp, cp, vp, sz, ip, ip, ip, ip, ip, ip, dp, vp,
+                                   ctypes.POINTER(ctypes.c_longlong)]
+        lib.refx_bench.restype = ip
     _ref[flavour] = lib
     return lib
+
+
+def host_threads():
+    """Threads for the reference's CPU work: every logical CPU this process
+    may use."""
+    return cpu_info()["logical_cpus"]
 
 
 def fec_params(short_frame, rate):
@@ -279,6 +362,21 @@ class OrcCode:
 class RefCode:
     """The reference decoder compiled from its own sources."""
 
+    def bench(self, pool, max_iter, threads, steps=1, calls_per_step=1, seconds=0.0, lanes=None):
+        """The reference's production mode on `pool` (int8 frames): worker
+        threads with their own handles decoding `lanes`-frame calls
+        (refbench.c).  Returns (seconds of every step, calls made)."""
+        lanes = lanes or self.lanes
+        pool = np.ascontiguousarray(pool, dtype=np.int8)
+        nsteps = 1 if seconds > 0 else steps
+        step_s = np.zeros(nsteps, np.float64)
+        calls = ctypes.c_longlong()
+        if self.lib.refx_bench(ctypes.byref(self.params), self.rate.encode(), pool.ctypes.data, pool.strides[0],
+                               pool.shape[0], max_iter, lanes, threads, steps, calls_per_step, float(seconds),
+                               step_s.ctypes.data, ctypes.byref(calls)):
+            raise RuntimeError("reference benchmark failed")
+        return step_s, calls.value
+
     def __init__(self, short_frame, rate, flavour=None, params=None):
         self.lib = load_ref(flavour)
         if self.lib is None:
@@ -289,6 +387,8 @@ class RefCode:
         self.h = self.lib.ref_ldpc_new(ctypes.byref(self.params), rate.encode())
         if not self.h:
             raise KeyError(rate)
+        self.rate = rate
+        self.flavour = flavour or best_ref_flavour()
         self.N = self.params.nldpc
         self.nbytes = (self.params.kldpc + 7) // 8
 
@@ -319,6 +419,34 @@ class RefCode:
             it[f] = max_iter if r < 0 else r
             ok[f] = r >= 0
         return out, it, ok
+
+    def decode_frames_mt(self, llr, max_iter, threads=None):
+        """Per-frame semantics (one call per frame) on host threads, each
+        with its own handle (refbench.c): hard bits, iterations, flags."""
+        llr = np.ascontiguousarray(llr, dtype=np.int8)
+        n = llr.shape[0]
+        out = np.zeros((n, self.nbytes), np.uint8)
+        it = np.zeros(n, np.int32)
+        ok = np.zeros(n, np.uint8)
+        if n and self.lib.refx_decode_frames_mt(ctypes.byref(self.params), self.rate.encode(), llr.ctypes.data,
+                                                llr.strides[0], n, max_iter, out.ctypes.data, out.strides[0],
+                                                it.ctypes.data, ok.ctypes.data, threads or host_threads()):
+            raise RuntimeError("reference per-frame decode failed")
+        return out, it, ok
+
+    def decode_groups_mt(self, llr, max_iter, group=None, threads=None):
+        """Consecutive groups of ``group`` frames (default: lanes), one call
+        each, on host threads: hard bits and the per-group return values."""
+        group = group or self.lanes
+        llr = np.ascontiguousarray(llr, dtype=np.int8)
+        n = llr.shape[0]
+        out = np.zeros((n, self.nbytes), np.uint8)
+        rets = np.zeros((n + group - 1) // group, np.int32)
+        if n and self.lib.refx_decode_groups_mt(ctypes.byref(self.params), self.rate.encode(), llr.ctypes.data,
+                                                llr.strides[0], n, group, max_iter, out.ctypes.data,
+                                                out.strides[0], rets.ctypes.data, threads or host_threads()):
+            raise RuntimeError("reference group decode failed")
+        return out, rets
 
     def decode_groups(self, llr, max_iter, group=None):
         """Consecutive groups of ``group`` (default: lanes) frames, one call

@@ -292,7 +292,9 @@ def test_pair_matches_frame_high_degree(short, rate, es, crate):
 def test_pair_matches_frame_every_code(short, rate):
     """Every code of both frame sizes: on 256 frames near the waterfall the
     frame-pair kernel gives the one-frame kernel's bits, iterations and flags,
-    with per-frame stopping and with group stopping (64-frame groups)."""
+    with per-frame stopping and with group stopping (64-frame groups), and
+    both give the reference's: each of the 256 frames decoded on its own and
+    two 64-frame calls (reference batch semantics)."""
     import re
 
     import torch
@@ -318,3 +320,14 @@ def test_pair_matches_frame_every_code(short, rate):
     for a, b in zip(res[D.VARIANT_FRAME], res[D.VARIANT_PAIR]):
         assert np.array_equal(a, b), rate
     d.close()
+    # and the reference itself: all 256 frames one call each, the first 128 in two 64-frame calls
+    import oracle
+    if oracle.ref_available("avx2"):
+        rb, ri, ro = oracle.RefCode(short, rate, flavour="avx2").decode_frames_mt(llr.cpu().numpy(), 30)
+        bits, it, ok = res[D.VARIANT_PAIR][:3]
+        assert np.array_equal(bits, rb) and np.array_equal(it, ri) and np.array_equal(ok, ro), rate
+    if oracle.ref_available("avx512"):
+        gb, rets = oracle.RefCode(short, rate, flavour="avx512").decode_groups_mt(host, 30, group=64)
+        bits, it, ok = res[D.VARIANT_PAIR][3:]
+        assert np.array_equal(bits, gb), rate
+        assert [int(it[g]) if ok[g:g + 64].all() else -1 for g in (0, 64)] == rets.tolist(), rate

@@ -58,6 +58,12 @@ EXPORTS = (
 )
 
 
+def test_fail_device_alloc(after):
+    """``drx_test_fail_device_alloc`` (testing): the library's next device
+    allocation after `after` more fails once; -1 turns it off."""
+    lib().drx_test_fail_device_alloc(int(after))
+
+
 def lib():
     """The loaded C-ABI library (raises if it has not been built)."""
     global _lib
@@ -99,6 +105,27 @@ def lib():
         L.drx_ldpc_mix_run.restype = ip
         L.drx_ldpc_set_variant.argtypes = [vp, ip]
         L.drx_ldpc_set_variant.restype = ip
+        L.drx_fec_decode_device.argtypes = [vp, vp, vp, sz, vp, sz, vp, vp, vp, ip, ip, ip, vp]
+        L.drx_fec_decode_device.restype = ip
+        L.drx_rxq_new.argtypes = [ip, ctypes.POINTER(FecParams), ctypes.POINTER(cp), ip, ip, ip, ip, ip]
+        L.drx_rxq_new.restype = vp
+        L.drx_rxq_free.argtypes = [vp]
+        L.drx_rxq_push.argtypes = [vp, ip, vp, ctypes.POINTER(ctypes.c_uint64)]
+        L.drx_rxq_push.restype = ip
+        L.drx_rxq_flush.argtypes = [vp]
+        L.drx_rxq_flush.restype = ip
+        L.drx_rxq_pop.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ip), vp,
+                                  ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                  ctypes.POINTER(ctypes.c_int32)]
+        L.drx_rxq_pop.restype = ip
+        L.drx_rxq_pending.argtypes = [vp]
+        L.drx_rxq_pending.restype = ip
+        L.drx_ldpc_set_wait_limit.argtypes = [vp, ip]
+        L.drx_ldpc_set_wait_limit.restype = ip
+        L.drx_ldpc_test_skip_vote.argtypes = [vp, ip]
+        L.drx_ldpc_test_skip_vote.restype = ip
+        L.drx_test_fail_device_alloc.argtypes = [ip]
+        L.drx_test_fail_device_alloc.restype = None
         L.drx_ldpc_device_error.argtypes = [vp]
         L.drx_ldpc_device_error.restype = ip
         L.drx_bb_descramble_device.argtypes = [vp, sz, ip, ip, vp]
@@ -283,7 +310,21 @@ class Ldpc:
         return r
 
     def device_error(self):
+        """``drx_ldpc_device_error``: the device error word since the last
+        call (0 fine, 2 a group barrier gave up), cleared."""
         return self._lib.drx_ldpc_device_error(self.h)
+
+    def set_wait_limit(self, polls):
+        """``drx_ldpc_set_wait_limit``: polls of a group barrier before a
+        group-stopping launch gives up (0: the default)."""
+        if self._lib.drx_ldpc_set_wait_limit(self.h, int(polls)) != 0:
+            raise ValueError(last_error())
+
+    def test_skip_vote(self, cta):
+        """``drx_ldpc_test_skip_vote`` (testing): CTA `cta` of later
+        group-stopping launches never votes; -1 turns it off."""
+        if self._lib.drx_ldpc_test_skip_vote(self.h, int(cta)) != 0:
+            raise ValueError(last_error())
 
     def set_learned(self, scale, offset, class_of_degree):
         """``drx_ldpc_set_learned``: scale and offset tables [iters, nclass]
@@ -555,3 +596,78 @@ class LdpcMix:
         s = stream if stream is not None else torch.cuda.current_stream()
         if self._lib.drx_ldpc_mix_run(self.h, stream_handle(s)) != 0:
             raise RuntimeError("drx_ldpc_mix_run: " + last_error())
+
+
+def fec_decode_device(dec, bch, llr, max_iter, stop=STOP_FRAME, stream=None):
+    """``drx_fec_decode_device``: LDPC then BCH of device rows (torch CUDA
+    int8 [n, >= nldpc]); returns (codewords uint8 [n, kldpc/8] corrected in
+    place by the BCH decoder, LDPC iterations, LDPC flags, BCH results)."""
+    import torch
+
+    n = llr.shape[0]
+    dev = llr.device
+    cw = torch.empty((n, dec.nbytes), dtype=torch.uint8, device=dev)
+    it = torch.empty(n, dtype=torch.int32, device=dev)
+    ok = torch.empty(n, dtype=torch.uint8, device=dev)
+    res = torch.empty(n, dtype=torch.int32, device=dev)
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    r = lib().drx_fec_decode_device(dec.h, bch.h, llr.data_ptr(), llr.stride(0), cw.data_ptr(), cw.stride(0),
+                                    it.data_ptr(), ok.data_ptr(), res.data_ptr(), n, int(max_iter), int(stop),
+                                    stream_handle(s))
+    if r != 0:
+        raise RuntimeError("drx_fec_decode_device: " + last_error())
+    return cw, it, ok, res
+
+
+class RxQueue:
+    """``drx_rxq_*``: the receiver's frame queue in front of the GPU.  codes:
+    sequence of (FecParams, rate); frames pushed with a code index come back
+    in arrival order, LDPC- and BCH-decoded."""
+
+    def __init__(self, codes, batch_frames=64, max_open=4, max_iter=30, group=False, max_latency_ms=0):
+        self._lib = lib()
+        params = (FecParams * len(codes))(*[FecParams(p.short_frame, p.nldpc, p.kldpc, p.kbch, p.t)
+                                             for p, _ in codes])
+        rates = (ctypes.c_char_p * len(codes))(*[r.encode() for _, r in codes])
+        self.nbytes = [(p.kldpc + 7) // 8 for p, _ in codes]
+        self.h = self._lib.drx_rxq_new(len(codes), params, rates, int(batch_frames), int(max_open), int(max_iter),
+                                       1 if group else 0, int(max_latency_ms))
+        if not self.h:
+            raise RuntimeError("drx_rxq_new: " + last_error())
+        self._buf = np.zeros(64800 // 8, np.uint8)
+
+    def push(self, code, llr):
+        """Queue one frame (host int8 [nldpc]); returns its sequence number."""
+        llr = np.ascontiguousarray(llr, dtype=np.int8)
+        f = ctypes.c_uint64()
+        if self._lib.drx_rxq_push(self.h, int(code), llr.ctypes.data, ctypes.byref(f)) != 0:
+            raise RuntimeError("drx_rxq_push: " + last_error())
+        return f.value
+
+    def flush(self):
+        if self._lib.drx_rxq_flush(self.h) != 0:
+            raise RuntimeError("drx_rxq_flush: " + last_error())
+
+    def pop(self, wait=True):
+        """The next frame in arrival order: (fseq, code, codeword bytes,
+        LDPC iterations, LDPC flag, BCH result), or None."""
+        f, c = ctypes.c_uint64(), ctypes.c_int()
+        it, ok, bch = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        r = self._lib.drx_rxq_pop(self.h, 1 if wait else 0, ctypes.byref(f), ctypes.byref(c), self._buf.ctypes.data,
+                                  ctypes.byref(it), ctypes.byref(ok), ctypes.byref(bch))
+        if r < 0:
+            raise RuntimeError("drx_rxq_pop: " + last_error())
+        if r == 0:
+            return None
+        return f.value, c.value, self._buf[: self.nbytes[c.value]].copy(), it.value, ok.value, bch.value
+
+    def pending(self):
+        return self._lib.drx_rxq_pending(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.drx_rxq_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -347,8 +347,8 @@ bool bch_scratch(drx_bch* b, size_t n)
     b->loc = nullptr;
     b->queue = nullptr;
     b->cap = 0;
-    if (!cuda_check(cudaMalloc(&b->loc, n * 16 * sizeof(uint16_t)), "cudaMalloc(bch)") ||
-        !cuda_check(cudaMalloc(&b->queue, n * sizeof(int32_t)), "cudaMalloc(bch)"))
+    if (!cuda_check(drxg::dev_malloc(&b->loc, n * 16 * sizeof(uint16_t)), "cudaMalloc(bch)") ||
+        !cuda_check(drxg::dev_malloc(&b->queue, n * sizeof(int32_t)), "cudaMalloc(bch)"))
         return false;
     b->cap = n;
     return true;
@@ -410,10 +410,10 @@ drx_bch* drx_bch_new(const drx_fec_params* p)
               cuda_check(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device), "attribute") &&
               cuda_check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     const size_t o_ex = tab.size() * 8, o_lg = o_ex + ex.size() * 2, total = o_lg + lg.size() * 2 + 64;
-    ok = ok && cuda_check(cudaMalloc(&b->blob, total), "cudaMalloc(bch tables)") &&
-         cuda_check(cudaMalloc(&b->count, sizeof(int)), "cudaMalloc") &&
-         cuda_check(cudaMalloc(&b->d_cw, (size_t)b->nbch / 8), "cudaMalloc") &&
-         cuda_check(cudaMalloc(&b->d_res, sizeof(int32_t)), "cudaMalloc");
+    ok = ok && cuda_check(drxg::dev_malloc(&b->blob, total), "cudaMalloc(bch tables)") &&
+         cuda_check(drxg::dev_malloc(&b->count, sizeof(int)), "cudaMalloc") &&
+         cuda_check(drxg::dev_malloc(&b->d_cw, (size_t)b->nbch / 8), "cudaMalloc") &&
+         cuda_check(drxg::dev_malloc(&b->d_res, sizeof(int32_t)), "cudaMalloc");
     if (ok) {
         char* base = (char*)b->blob;
         ok = cuda_check(cudaMemcpy(base, tab.data(), o_ex, cudaMemcpyHostToDevice), "cudaMemcpy") &&

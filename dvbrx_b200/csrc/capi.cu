@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -79,10 +80,10 @@ bool ensure_stage(drx_ldpc* d, size_t nframes)
         !cuda_ok(cudaMallocHost(&d->h_out, nframes * nb), "cudaMallocHost") ||
         !cuda_ok(cudaMallocHost(&d->h_it, nframes * 4), "cudaMallocHost") ||
         !cuda_ok(cudaMallocHost(&d->h_ok, nframes), "cudaMallocHost") ||
-        !cuda_ok(cudaMalloc(&d->d_llr, nframes * N), "cudaMalloc") ||
-        !cuda_ok(cudaMalloc(&d->d_out, nframes * nb), "cudaMalloc") ||
-        !cuda_ok(cudaMalloc(&d->d_it, nframes * 4), "cudaMalloc") ||
-        !cuda_ok(cudaMalloc(&d->d_ok, nframes), "cudaMalloc")) {
+        !cuda_ok(drxg::dev_malloc(&d->d_llr, nframes * N), "cudaMalloc") ||
+        !cuda_ok(drxg::dev_malloc(&d->d_out, nframes * nb), "cudaMalloc") ||
+        !cuda_ok(drxg::dev_malloc(&d->d_it, nframes * 4), "cudaMalloc") ||
+        !cuda_ok(drxg::dev_malloc(&d->d_ok, nframes), "cudaMalloc")) {
         release_stage(d);
         return false;
     }
@@ -98,7 +99,7 @@ bool ensure_scratch(drx_ldpc* d, size_t need)
     cudaFree(d->msg);
     d->msg = nullptr;
     d->msg_cap = 0;
-    if (!cuda_ok(cudaMalloc(&d->msg, need), "cudaMalloc(messages)"))
+    if (!cuda_ok(drxg::dev_malloc(&d->msg, need), "cudaMalloc(messages)"))
         return false;
     d->msg_cap = need;
     return true;
@@ -122,7 +123,7 @@ bool ensure_msg(drx_ldpc* d, int grid)
     cudaFree(d->msg);
     d->msg = nullptr;
     d->msg_cap = 0;
-    if (!cuda_ok(cudaMalloc(&d->msg, need), "cudaMalloc(messages)"))
+    if (!cuda_ok(drxg::dev_malloc(&d->msg, need), "cudaMalloc(messages)"))
         return false;
     d->msg_cap = need;
     return true;
@@ -136,7 +137,7 @@ bool ensure_sync(drx_ldpc* d, size_t words)
     cudaFree(d->sync);
     d->sync = nullptr;
     d->sync_cap = 0;
-    if (!cuda_ok(cudaMalloc(&d->sync, words * sizeof(unsigned)), "cudaMalloc(sync)"))
+    if (!cuda_ok(drxg::dev_malloc(&d->sync, words * sizeof(unsigned)), "cudaMalloc(sync)"))
         return false;
     d->sync_cap = words;
     return true;
@@ -155,7 +156,7 @@ bool upload_code(drx_ldpc* d)
     const size_t o_nlev = o_lmeta + a16(c.lmeta.size() * sizeof(uint64_t));
     const size_t total = o_nlev + a16(c.nlev.size());
     std::vector<char> host(total, 0);
-    if (!cuda_ok(cudaMalloc(&d->blob, total), "cudaMalloc(code)"))
+    if (!cuda_ok(drxg::dev_malloc(&d->blob, total), "cudaMalloc(code)"))
         return false;
     char* base = (char*)d->blob;
     DevCode dc{};
@@ -233,6 +234,8 @@ int enqueue(drx_ldpc* d, const int8_t* llr, size_t llr_stride, uint8_t* out, siz
     p.nframes = nframes;
     p.max_iter = max_iter;
     p.err = d->err;
+    p.wait_limit = d->wait_limit;
+    p.skip_vote = d->test_skip_vote;
     if (x) {
         if (stop != 0) {
             set_err("learned check nodes and row lists need per-frame stopping");
@@ -336,7 +339,7 @@ bool ensure_pipe(drx_ldpc* d)
         return true;
     bool ok = cuda_ok(cudaStreamCreateWithFlags(&d->pipe[0], cudaStreamNonBlocking), "cudaStreamCreate") &&
               cuda_ok(cudaStreamCreateWithFlags(&d->pipe[1], cudaStreamNonBlocking), "cudaStreamCreate") &&
-              cuda_ok(cudaMalloc(&d->chunk_work, kMaxChunks * sizeof(unsigned)), "cudaMalloc");
+              cuda_ok(drxg::dev_malloc(&d->chunk_work, kMaxChunks * sizeof(unsigned)), "cudaMalloc");
     for (int k = 0; ok && k < kChunkEvents; k++)
         ok = cuda_ok(cudaEventCreateWithFlags(&d->chunk_ev[k], cudaEventDisableTiming), "cudaEventCreate");
     if (ok)
@@ -360,7 +363,7 @@ bool ensure_msg2(drx_ldpc* d, size_t need)
     cudaFree(d->msg2);
     d->msg2 = nullptr;
     d->msg2_cap = 0;
-    if (!cuda_ok(cudaMalloc(&d->msg2, need), "cudaMalloc(messages)"))
+    if (!cuda_ok(drxg::dev_malloc(&d->msg2, need), "cudaMalloc(messages)"))
         return false;
     d->msg2_cap = need;
     return true;
@@ -521,18 +524,57 @@ bool ensure_fallback(drx_ldpc* d, size_t nframes)
     d->fb_rows = nullptr;
     d->fb_ok = nullptr;
     d->fb_cap = 0;
-    if (!cuda_ok(cudaMalloc(&d->fb_rows, nframes * sizeof(int32_t) + 16), "cudaMalloc(fallback rows)") ||
-        !cuda_ok(cudaMalloc(&d->fb_ok, nframes), "cudaMalloc(fallback flags)"))
+    if (!cuda_ok(drxg::dev_malloc(&d->fb_rows, nframes * sizeof(int32_t) + 16), "cudaMalloc(fallback rows)") ||
+        !cuda_ok(drxg::dev_malloc(&d->fb_ok, nframes), "cudaMalloc(fallback flags)"))
         return false;
     d->fb_cap = nframes;
     return true;
 }
 
+/* allocation-failure test hook: allocations left before one fails (-1: off) */
+std::atomic<long> g_alloc_countdown{ -1 };
+
 }  // namespace
+
+namespace drxg {
+
+bool alloc_fails_now()
+{
+    long v = g_alloc_countdown.load();
+    while (v >= 0) {
+        if (g_alloc_countdown.compare_exchange_weak(v, v - 1))
+            return v == 0;
+    }
+    return false;
+}
+
+}  // namespace drxg
 
 extern "C" {
 
 const char* drx_ldpc_last_error(void) { return g_err.c_str(); }
+
+void drx_test_fail_device_alloc(int after) { g_alloc_countdown.store(after < 0 ? -1 : after); }
+
+int drx_ldpc_set_wait_limit(drx_ldpc* d, int polls)
+{
+    if (!d || polls < 0) {
+        set_err("drx_ldpc_set_wait_limit: NULL handle or negative limit");
+        return -1;
+    }
+    d->wait_limit = polls;
+    return 0;
+}
+
+int drx_ldpc_test_skip_vote(drx_ldpc* d, int cta)
+{
+    if (!d || cta < -1) {
+        set_err("drx_ldpc_test_skip_vote: NULL handle or CTA below -1");
+        return -1;
+    }
+    d->test_skip_vote = cta + 1;
+    return 0;
+}
 
 int drx_fec_lookup(int short_frame, const char* rate, drx_fec_params* p)
 {
@@ -582,8 +624,8 @@ drx_ldpc* drx_ldpc_new(const drx_fec_params* p, const char* rate)
         !cuda_ok(cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount, d->device),
                  "cudaDeviceGetAttribute") ||
         !cuda_ok(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "cudaStreamCreate") ||
-        !upload_code(d) || !cuda_ok(cudaMalloc(&d->work, 256), "cudaMalloc") ||
-        !cuda_ok(cudaMalloc(&d->err, sizeof(int)), "cudaMalloc") ||
+        !upload_code(d) || !cuda_ok(drxg::dev_malloc(&d->work, 256), "cudaMalloc") ||
+        !cuda_ok(drxg::dev_malloc(&d->err, sizeof(int)), "cudaMalloc") ||
         !cuda_ok(cudaMemset(d->err, 0, sizeof(int)), "cudaMemset")) {
         drx_ldpc_free(d);
         return nullptr;
@@ -771,7 +813,7 @@ int drx_ldpc_set_learned(drx_ldpc* d, int iters, int nclass, const int8_t* class
             tab[(size_t)t * kLearnClasses + k] = (uint32_t)bq | (uint32_t)(uint16_t)(int16_t)aq << 16;
         }
     if (!d->learn) {
-        if (!cuda_ok(cudaMalloc(&d->learn, sizeof(uint32_t) * kLearnMaxIters * kLearnClasses + 64),
+        if (!cuda_ok(drxg::dev_malloc(&d->learn, sizeof(uint32_t) * kLearnMaxIters * kLearnClasses + 64),
                      "cudaMalloc(learned table)"))
             return -1;
     }

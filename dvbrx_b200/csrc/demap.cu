@@ -404,9 +404,9 @@ drx_demapper* drx_demapper_new(const char* constellation, const char* rate, int 
     if (!cuda_check(cudaGetDevice(&m->device), "cudaGetDevice") ||
         !cuda_check(cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, m->device), "attribute") ||
         !cuda_check(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate") ||
-        !cuda_check(cudaMalloc(&m->d_sym, sizeof(float) * 2 * (size_t)p.nsym), "cudaMalloc") ||
-        !cuda_check(cudaMalloc(&m->d_n0, sizeof(float)), "cudaMalloc") ||
-        !cuda_check(cudaMalloc(&m->d_llr, (size_t)p.nldpc), "cudaMalloc")) {
+        !cuda_check(drxg::dev_malloc(&m->d_sym, sizeof(float) * 2 * (size_t)p.nsym), "cudaMalloc") ||
+        !cuda_check(drxg::dev_malloc(&m->d_n0, sizeof(float)), "cudaMalloc") ||
+        !cuda_check(drxg::dev_malloc(&m->d_llr, (size_t)p.nldpc), "cudaMalloc")) {
         drx_demapper_free(m);
         return nullptr;
     }

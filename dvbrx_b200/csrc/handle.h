@@ -32,6 +32,8 @@ struct drx_ldpc {
     int pair_ctas_per_sm = 0; /* 0: the frame-pair kernel does not run this code */
     int pair_kid = -1;        /* its instantiation for this code */
     int variant = DRX_VARIANT_AUTO;
+    int wait_limit = 0;     /* polls of a group barrier before a launch gives up (0: default) */
+    int test_skip_vote = 0; /* testing: CTA test_skip_vote - 1 of group launches never votes */
     cudaStream_t stream = nullptr;
     /* scratch */
     void* msg = nullptr;
@@ -73,5 +75,21 @@ namespace drxg {
 
 void set_error(const std::string& s);
 bool cuda_check(cudaError_t e, const char* what);
+
+/* True if the next device allocation of the library must fail (the
+ * allocation-failure test hook, drx_test_fail_device_alloc). */
+bool alloc_fails_now();
+
+/* cudaMalloc through the library's test hook: every device allocation of
+ * the library goes through here. */
+template <class T>
+cudaError_t dev_malloc(T** p, size_t n)
+{
+    if (alloc_fails_now()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc((void**)p, n);
+}
 
 }  // namespace drxg

@@ -40,7 +40,6 @@
 namespace drxg {
 
 constexpr int kQC = 360;
-constexpr int kSpinLimit = 1 << 22; /* polls of a group barrier before giving up */
 
 /* One 32-bit word per check up to degree 16 (6 + 6 + 4 bits, 16 signs),
  * two above (6 + 6 + 5 bits, 32 signs). */
@@ -321,30 +320,36 @@ __device__ void store_bits(const DevCode& c, const Frame& fr, uint8_t* __restric
 }
 
 /* Group barrier of a team of G co-resident CTAs: returns 1 if every member
- * passed its syndrome, 0 if not, -1 if the barrier timed out. */
-__device__ int team_vote(unsigned* slot, int G, bool fail, int* err)
+ * passed its syndrome, 0 if not, -1 if the barrier timed out after `limit`
+ * polls (the device error word is set to 2).  skip: this CTA does not
+ * arrive (a test of the time-out) and returns -1. */
+__device__ int team_vote(unsigned* slot, int G, bool fail, int* err, int limit, bool skip)
 {
     __shared__ int s_res;
     if (threadIdx.x == 0) {
         unsigned* arrive = slot;
         unsigned* fails = slot + 1;
-        if (fail)
-            atomicAdd(fails, 1u);
-        __threadfence();
-        atomicAdd(arrive, 1u);
-        int spins = 0;
         int res = 0;
-        while (*(volatile unsigned*)arrive < (unsigned)G) {
-            if (++spins > kSpinLimit) {
-                atomicExch(err, 2);
-                res = -1;
-                break;
+        if (skip) {
+            res = -1;
+        } else {
+            if (fail)
+                atomicAdd(fails, 1u);
+            __threadfence();
+            atomicAdd(arrive, 1u);
+            int spins = 0;
+            while (*(volatile unsigned*)arrive < (unsigned)G) {
+                if (++spins > limit) {
+                    atomicExch(err, 2);
+                    res = -1;
+                    break;
+                }
+                __nanosleep(200);
             }
-            __nanosleep(200);
+            __threadfence();
+            if (res == 0)
+                res = *(volatile unsigned*)fails == 0 ? 1 : 0;
         }
-        __threadfence();
-        if (res == 0)
-            res = *(volatile unsigned*)fails == 0 ? 1 : 0;
         s_res = res;
     }
     __syncthreads();
@@ -371,7 +376,9 @@ __device__ __forceinline__ void decode_frame(const DevCode& c, const Frame& fr, 
         if (threadIdx.x == 0)
             *sflag = 0; /* read again only after later barriers */
         if (sync) {
-            const int v = team_vote(sync + 2 * it, p.group, fail, p.err);
+            const int v = team_vote(sync + 2 * it, p.group, fail, p.err,
+                                    p.wait_limit > 0 ? p.wait_limit : kDefaultWaitLimit,
+                                    (int)blockIdx.x + 1 == p.skip_vote);
             ok = v == 1;
             if (v < 0)
                 break;

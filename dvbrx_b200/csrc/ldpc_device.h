@@ -51,7 +51,14 @@ struct DecodeParams {
                               rows of kLearnClasses words, see learned_mag */
     const int8_t* learn_class; /* degree class of every check degree 0..32 */
     int learn_iters;
+    int wait_limit;        /* group mode: polls of a group barrier before the launch gives
+                              up and sets the error word to 2 (0: kDefaultWaitLimit) */
+    int skip_vote;         /* group mode, testing only: CTA skip_vote - 1 never arrives at
+                              its team's barriers (the others time out); 0: none */
 };
+
+/* Polls of a group barrier (about 200 ns apart) before it gives up. */
+constexpr int kDefaultWaitLimit = 1 << 22;
 
 /* Learned check nodes (the neural offset / scaled min-sum at int8): the
  * outgoing magnitude of a node in iteration t is

@@ -99,11 +99,23 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
  * (absent for (0, 0)), 2 + e information entry e of the layer.  DM is the
  * node degree (EXACT) or a bound on it (the degree is then a run-time
  * value).  The node state lives in registers across the phases of its layer
- * (see layer_pair).  Slot masks, sign bits and the message index keep slot
- * k at bit k.  The full passes run every slot without branches: a slot that
- * is not a link, or whose bit an earlier check of the layer writes (read
- * later, in its level), enters the minimums as 255, which no magnitude
- * reaches; stores are predicated.
+ * (see layer_pair).  Slot masks and the message index keep slot k at bit k.
+ *
+ * Minimums are taken over keys |x| * 32 + k (|x| <= 128, so a key fits 13
+ * bits of a 16-bit lane): the smallest key gives min0 and the slot holding
+ * it, the second smallest min1 (a tie between two slots at min0 puts min1 =
+ * min0, and then which slot holds min0 changes no message).  The full
+ * passes run every slot without branches: a slot that is not a link, or
+ * whose bit an earlier check of the layer writes (read later, in its level),
+ * enters the minimums with a key above every real one; stores are
+ * predicated.
+ *
+ * Sign bits of a record: the 16 slots of a word in the byte layout
+ * byte 0 = lane A even slots, byte 1 = lane A odd slots, byte 2 = lane B
+ * even slots, byte 3 = lane B odd slots, slot 2s (2s + 1) at bit 7 - s of
+ * its byte; shifted left by s, the word holds the signs of slots 2s and
+ * 2s + 1 in the sign bits of its bytes, which one PRMT turns into lane
+ * masks.
  */
 /* A check's message record: 8 bytes up to degree 16 (per lane min0, min1
  * and a 4-bit index in one word, 16 sign bits per lane in the other); 16
@@ -111,6 +123,21 @@ __device__ __forceinline__ uint32_t heq(uint32_t a, uint32_t b)
  * the index, 16 bits per lane). */
 template <bool WIDE>
 using PairRec = typename std::conditional<WIDE, uint4, uint2>::type;
+
+/* key of a slot that takes no part in the minimums */
+constexpr uint32_t kKeyOff = 0x1FE01FE0u; /* 255 * 32 in both lanes */
+
+/* the sign bits of slot k (k < 16) of both lanes in a record word */
+__device__ __forceinline__ constexpr uint32_t sign_bits(int k)
+{
+    return (k & 1) ? (1u << (15 - (k >> 1))) | (1u << (31 - (k >> 1)))
+                   : (1u << (7 - (k >> 1))) | (1u << (23 - (k >> 1)));
+}
+/* lane masks of slot k's sign bits in record word w (k < 16) */
+__device__ __forceinline__ uint32_t sign_mask(uint32_t w, int k)
+{
+    return prmt(w << (k >> 1), 0, (k & 1) ? 0xBB99u : 0xAA88u);
+}
 
 /* WIDE: the kernel's records are 16 bytes (its degree bound is above 16).
  * PO: the parity posteriors (slots 0 and 1) are not in shared memory; the
@@ -126,10 +153,13 @@ struct PairCheck {
     uint32_t addr[S]; /* shared-memory byte addresses of the owned links' posteriors */
     uint32_t x[S];
     uint32_t live, inm, outm; /* bit k: slot k is a link / is read late / is written early */
-    uint32_t n0, n1, p0, p1, idxh, sgn, sgn1; /* sgn: sign bits of slots 0-15, sgn1: 16-31 */
-    uint32_t min0, min1, sg, mn0, mn1;
-    uint32_t m0p1, nmn0, nmn1; /* min0 + 1, -mn0, -mn1 (set by finish) */
+    uint32_t n0, n1, p0, p1, idxh, sgn, sgn1; /* old messages; sgn: sign bits of slots 0-15, sgn1: 16-31 */
+    uint32_t min0, min1, sg;                  /* smallest keys, sign parity (bit 15 / 31) */
+    uint32_t a0, a1, b0, b1, nidx;            /* outgoing message candidates (set by finish), index */
+    uint32_t recw;                            /* the record's magnitude word (set by finish) */
 
+    /* ent: the layer's entries (shared byte address of the link group's first
+     * posterior word, -2a), cnt of them */
     __device__ __forceinline__ void setup(const int2* __restrict__ ent, int cnt, int K, int q, int i, int j,
                                           Rec rec, uint32_t fresh, unsigned long long meta, uint32_t sbase)
     {
@@ -142,14 +172,18 @@ struct PairCheck {
         live = lv;
         inm = (uint32_t)(meta >> 8) & 0xFFFFFFu;
         outm = (uint32_t)(meta >> 32) & 0xFFFFFFu;
+        const uint32_t tj = 2u * (uint32_t)j;
 #pragma unroll
         for (int k = 0; k < S; k++) {
             if (k < 2) {
                 addr[k] = PO ? 0u : sbase + 2u * (uint32_t)(k == 0 ? pc : pp);
             } else {
-                /* a slot past the degree takes the last link's address: read, never used */
+                /* a slot past the degree takes the last link's address: read, never used.
+                 * Link of check j: word (j - a) mod 360 of the group, as min(u, u + 720)
+                 * over unsigned byte offsets u = 2 j - 2 a */
                 const int2 e = ent[min(k, D - 1) - 2];
-                addr[k] = (uint32_t)e.x + 2u * (uint32_t)j + (j < e.y ? 2u * kQCp : 0u);
+                const uint32_t u = tj + (uint32_t)e.y;
+                addr[k] = (uint32_t)e.x + __viaddmin_u32(u, 2u * kQCp, u);
             }
         }
         /* messages: zero for a lane in its first iteration */
@@ -168,7 +202,7 @@ struct PairCheck {
         n1 = m1;
         p0 = __viaddmax_s16x2(~m0, 0x00010001u, 0xFFE1FFE1u); /* max(-m, -31) */
         p1 = __viaddmax_s16x2(~m1, 0x00010001u, 0xFFE1FFE1u);
-        min0 = min1 = 0x00FF00FFu;
+        min0 = min1 = kKeyOff;
         sg = 0;
     }
 
@@ -176,16 +210,20 @@ struct PairCheck {
     __device__ __forceinline__ uint32_t unmsg(int k) const
     {
         const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)k * 0x00010001u);
-        const uint32_t sm = lmask((k < 16 ? sgn : sgn1) << (15 - (k & 15)));
+        const uint32_t sm = sign_mask(k < 16 ? sgn : sgn1, k & 15);
         return sel(sm, sel(im, n1, n0), sel(im, p1, p0));
     }
 
-    __device__ __forceinline__ void fold(uint32_t v)
+    /* the key of value v in slot k */
+    static __device__ __forceinline__ uint32_t key(uint32_t v, int k)
     {
-        const uint32_t a = abs2(v);
-        min1 = __vmins2(min1, __vmaxs2(min0, a));
-        min0 = __vmins2(min0, a);
-        sg ^= v;
+        return abs2(v) * 32u + (uint32_t)k * 0x00010001u;
+    }
+
+    __device__ __forceinline__ void fold(uint32_t kv)
+    {
+        min1 = __vmins2(min1, __vmaxs2(min0, kv));
+        min0 = __vmins2(min0, kv);
     }
 
     /* every slot but the late ones, without branches; minimums folded
@@ -197,28 +235,38 @@ struct PairCheck {
     __device__ __forceinline__ void read_all(const uint16_t* __restrict__ post, uint32_t r0, uint32_t r1)
     {
         const uint32_t excl = LEV ? (~live | inm) : ~live;
-        uint32_t f[S];
-#pragma unroll
-        for (int k = 0; k < S; k++) {
+        /* slot k read: its value kept in x[k] (minus its old message for a
+         * late slot), its key returned */
+        auto slot = [&](int k) {
             const uint32_t m = unmsg(k);
             const uint32_t raw = PO && k < 2 ? (k == 0 ? r0 : r1) : lds16(addr[k]);
-            uint32_t v = sadd(sx2(raw), m);
-            if (LEV || !EXACT || k == 1)
-                v = ((excl >> k) & 1u) ? 0x00FF00FFu : v;
-            f[k] = v;
-            /* a late slot keeps minus its old message for read_late */
-            x[k] = LEV && ((inm >> k) & 1u) ? m : v;
-        }
+            const uint32_t v = sadd(sx2(raw), m);
+            uint32_t kv = key(v, k);
+            /* late slots are among K0 .. K1; past them only a non-link (inexact kernels) */
+            const bool maybe_late = LEV && k >= K0 && k <= K1;
+            if (maybe_late || !EXACT || k == 1) {
+                /* excluded: not a link, or late (its sign and key are taken in read_late) */
+                const bool ex = (excl >> k) & 1u;
+                kv = ex ? kKeyOff : kv;
+                sg ^= ex ? 0u : v;
+            } else {
+                sg ^= v;
+            }
+            if (maybe_late)
+                x[k] = ((inm >> k) & 1u) ? m : v;
+            else
+                x[k] = v;
+            return kv;
+        };
 #pragma unroll
         for (int k = 0; k + 1 < S; k += 2) {
-            const uint32_t a = abs2(f[k]), b = abs2(f[k + 1]);
+            const uint32_t a = slot(k), b = slot(k + 1);
             const uint32_t lo = __vmins2(a, b), hi = __vmaxs2(a, b);
             min1 = __vimin3_s16x2(__vmaxs2(min0, lo), min1, hi);
             min0 = __vimin3_s16x2(min0, a, b);
-            sg ^= f[k] ^ f[k + 1];
         }
         if (S & 1)
-            fold(f[S - 1]);
+            fold(slot(S - 1));
     }
 
     /* a thread that holds no check (t >= 360): valid addresses, no links, so
@@ -228,13 +276,13 @@ struct PairCheck {
 #pragma unroll
         for (int k = 0; k < S; k++) {
             addr[k] = sbase;
-            x[k] = 0x00FF00FFu;
+            x[k] = 0;
         }
         live = inm = outm = 0;
         n0 = n1 = p0 = p1 = sgn = sgn1 = 0;
         idxh = 0x64006400u;
-        min0 = min1 = 0x00FF00FFu;
-        sg = mn0 = mn1 = m0p1 = nmn0 = nmn1 = 0;
+        min0 = min1 = kKeyOff;
+        sg = a0 = a1 = b0 = b1 = nidx = recw = 0;
     }
 
     /* the late slots (their bits were written by earlier levels) of a check
@@ -250,44 +298,50 @@ struct PairCheck {
             const bool in = (im >> k) & 1u;
             const uint32_t v = sadd(sx2(lds16(addr[k])), x[k]);
             x[k] = in ? v : x[k];
-            fold(in ? v : 0x00FF00FFu);
+            sg ^= in ? v : 0u;
+            fold(in ? key(v, k) : kKeyOff);
         }
     }
 
     /* the cap at 127 and offset 1, or the learned scale and offset of each
-     * lane's iteration (lpA, lpB).  Only threads with `take` keep the result:
-     * the level steps run it on whole warps */
+     * lane's iteration (lpA, lpB); the outgoing candidates +-mn0, +-mn1 with
+     * the check's sign parity applied (a0, a1 for a slot whose value is
+     * positive, b0 = -a0, b1 = -a1 otherwise) and the record's magnitudes.
+     * Only threads with `take` keep the result: the level steps run it on
+     * whole warps */
     __device__ __forceinline__ void finish(bool take, bool learned, uint32_t lpA, uint32_t lpB)
     {
-        const uint32_t c1 = min1, c0 = min0;
+        const uint32_t c0 = __vmins2((min0 >> 5) & 0x07FF07FFu, 0x007F007Fu);
+        const uint32_t c1 = __vmins2((min1 >> 5) & 0x07FF07FFu, 0x007F007Fu);
         uint32_t m0, m1;
         if (learned) {
-            const uint32_t k0 = __vmins2(c0, 0x007F007Fu), k1 = __vmins2(c1, 0x007F007Fu);
-            m0 = (uint32_t)learned_mag(k0 & 0xFFFF, lpA) | (uint32_t)learned_mag(k0 >> 16, lpB) << 16;
-            m1 = (uint32_t)learned_mag(k1 & 0xFFFF, lpA) | (uint32_t)learned_mag(k1 >> 16, lpB) << 16;
+            m0 = (uint32_t)learned_mag(c0 & 0xFFFF, lpA) | (uint32_t)learned_mag(c0 >> 16, lpB) << 16;
+            m1 = (uint32_t)learned_mag(c1 & 0xFFFF, lpA) | (uint32_t)learned_mag(c1 >> 16, lpB) << 16;
         } else {
-            m0 = __viaddmax_s16x2(__vmins2(c0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
-            m1 = __viaddmax_s16x2(__vmins2(c1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+            m0 = __viaddmax_s16x2(c0, 0xFFFFFFFFu, 0u);
+            m1 = __viaddmax_s16x2(c1, 0xFFFFFFFFu, 0u);
         }
         if (take) {
-            mn0 = m0;
-            mn1 = m1;
-            m0p1 = __vadd2(c0, 0x00010001u);
-            nmn0 = neg2(m0);
-            nmn1 = neg2(m1);
+            const uint32_t sm = lmask(sg);
+            a0 = sel(sm, neg2(m0), m0);
+            a1 = sel(sm, neg2(m1), m1);
+            b0 = neg2(a0);
+            b1 = neg2(a1);
+            nidx = (min0 & 0x001F001Fu) | 0x64006400u; /* FP16 1024 + slot of min0 */
+            /* per lane min0 (6 bits) | min1 << 6, magnitudes capped at 32 (| index << 12 below degree 17) */
+            recw = __vmins2(m0, 0x00200020u) | (__vmins2(m1, 0x00200020u) << 6);
+            if (!WIDE)
+                recw |= (min0 & 0x000F000Fu) << 12;
         }
     }
 
-    /* new posterior of slot k (two bytes), and its masks: lanes where
-     * |x| is above min0 (the slot does not hold the minimum) and lanes whose
-     * outgoing message is negative */
-    __device__ __forceinline__ uint32_t update(int k, uint32_t& above, uint32_t& neg) const
+    /* new posterior of slot k (two bytes) and the lane mask of its value's sign */
+    __device__ __forceinline__ uint32_t update(int k, uint32_t& xm) const
     {
         const uint32_t v = x[k];
-        /* min0 - |x| = min(min0 + x, (min0 + 1) + ~x) < 0 */
-        above = lmask(__viaddmin_s16x2(~v, m0p1, __vadd2(min0, v)));
-        neg = lmask(sg ^ v);
-        const uint32_t o = sel(neg, sel(above, nmn0, nmn1), sel(above, mn0, mn1));
+        xm = lmask(v);
+        const uint32_t eq = heq(nidx, 0x64006400u + (uint32_t)k * 0x00010001u);
+        const uint32_t o = sel(xm, sel(eq, b1, b0), sel(eq, a1, a0));
         return pk2(sadd(v, o));
     }
 
@@ -299,47 +353,52 @@ struct PairCheck {
         const uint32_t om = mine ? outm : 0u;
 #pragma unroll
         for (int k = K0; k <= KE; k++) {
-            uint32_t above, neg;
-            const uint32_t nv = update(k, above, neg);
+            uint32_t xm;
+            const uint32_t nv = update(k, xm);
             if ((om >> k) & 1u)
                 sts16(addr[k], nv);
         }
     }
 
     /* every other posterior (predicated stores) and the node's compressed
-     * messages for both lanes, stored by thread 0: the slot holding min0 and
-     * one sign bit per slot.  PO: the parity words go to o0 and o1. */
+     * messages for both lanes: the slot holding min0 and one sign bit per
+     * slot (the outgoing message's: the value's sign times the parity).
+     * PO: the parity words go to o0 and o1. */
     __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, Rec* __restrict__ dst, uint32_t& o0,
                                                uint32_t& o1)
     {
         const uint32_t wm = live & ~outm;
-        uint32_t nidx = 0, nsg = 0, nsg1 = 0; /* nidx per lane: k + 1 of a slot holding min0, 0 if none */
+        uint32_t nsg = 0, nsg1 = 0;
 #pragma unroll
         for (int k = 0; k < S; k++) {
-            uint32_t above, neg;
-            const uint32_t nv = update(k, above, neg);
+            uint32_t xm;
+            const uint32_t nv = update(k, xm);
             if (PO && k < 2)
                 (k == 0 ? o0 : o1) = nv;
+            else if (EXACT && k > K1 && k != 1)
+                sts16(addr[k], nv); /* every slot past K1 is a link written here */
             else if ((wm >> k) & 1u)
                 sts16(addr[k], nv);
-            nidx = sel(above, nidx, (uint32_t)(k + 1) * 0x00010001u);
             if (k < 16)
-                nsg |= neg & (0x00010001u << k);
+                nsg |= xm & sign_bits(k);
             else
-                nsg1 |= neg & (0x00010001u << (k - 16));
+                nsg1 |= xm & sign_bits(k - 16);
         }
-        nidx = __viaddmax_s16x2(nidx, 0xFFFFFFFFu, 0u); /* slot number: max(nidx - 1, 0) */
-        const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
-        if constexpr (WIDE)
-            __stcg(dst, make_uint4(m0c | (m1c << 6), nsg, nsg1, nidx));
-        else
-            __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
+        /* the outgoing signs: each value's sign flipped where the parity is odd */
+        const uint32_t pm = lmask(sg);
+        nsg ^= pm;
+        if constexpr (WIDE) {
+            nsg1 ^= pm;
+            __stcg(dst, make_uint4(recw, nsg, nsg1, nidx & 0x001F001Fu));
+        } else {
+            __stcg(dst, make_uint2(recw, nsg));
+        }
     }
 };
 
 struct PairFrame {
     uint16_t* post;
-    const int2* ent; /* (shared byte address of the link for check 0 before the wrap, a) */
+    const int2* ent; /* (shared byte address of the link group's first word, -2 a) */
     const uint16_t* eoff;
     const uint32_t* steps;
     /* parity out of shared memory (PO kernels): the posterior word of
@@ -368,12 +427,13 @@ __device__ PairFrame stage_pair(const DevCode& c, char* smem, uint16_t* gpar)
     uint16_t* eoff = (uint16_t*)(smem + off);
     off += a16p(sizeof(uint16_t) * (c.q + 1));
     uint32_t* steps = (uint32_t*)(smem + off);
-    /* entries as shared byte addresses: x = posterior address of link (g, a)
-     * for check 0, before the wrap (link of check j: x + 2 j, + 720 if j < a) */
+    /* entries (360 g - a, a) as (shared byte address of group g's first
+     * posterior word, -2 a): the link of check j is word (j - a) mod 360 of
+     * the group, at byte offset min(u, u + 720), u = 2 j - 2 a unsigned */
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(f.post);
     for (int k = threadIdx.x; k < c.nent; k += blockDim.x) {
         const int2 e = c.ent[k];
-        ent[k] = make_int2((int)(sbase + 2u * (uint32_t)e.x), e.y);
+        ent[k] = make_int2((int)(sbase + 2u * (uint32_t)(e.x + e.y)), -2 * e.y);
     }
     for (int k = threadIdx.x; k <= c.q; k += blockDim.x)
         eoff[k] = c.eoff[k];
@@ -492,7 +552,8 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
                 const int e1 = fr.eoff[i + 1];
                 for (int e = fr.eoff[i]; e < e1; e++) {
                     const int2 en = fr.ent[e];
-                    const uint32_t v = sx2(lds16((uint32_t)en.x + 2u * (uint32_t)j + (j < en.y ? 2u * kQCp : 0u)));
+                    const uint32_t u = 2u * (uint32_t)j + (uint32_t)en.y;
+                    const uint32_t v = sx2(lds16((uint32_t)en.x + __viaddmin_u32(u, 2u * kQCp, u)));
                     par ^= v;
                     z |= __vadd2(v, 0xFFFFFFFFu) & ~v;
                 }
@@ -678,30 +739,35 @@ static __device__ void store_lane(const DevCode& c, const PairFrame& fr, int h, 
 
 /* Group barrier of a team of M co-resident CTAs (a cooperative launch):
  * returns 1 if no member saw a failing frame, 0 if one did, -1 if the
- * barrier gave up after kPairSpinLimit polls (the device error word is set). */
-constexpr int kPairSpinLimit = 1 << 22;
-static __device__ int pair_team_vote(unsigned* slot, int M, bool fail, int* err)
+ * barrier gave up after `limit` polls (the device error word is set to 2).
+ * skip: this CTA does not arrive (a test of the time-out) and returns -1. */
+static __device__ int pair_team_vote(unsigned* slot, int M, bool fail, int* err, int limit, bool skip)
 {
     __shared__ int s_res;
     if (threadIdx.x == 0) {
         unsigned* arrive = slot;
         unsigned* fails = slot + 1;
-        if (fail)
-            atomicAdd(fails, 1u);
-        __threadfence();
-        atomicAdd(arrive, 1u);
-        int spins = 0, res = 0;
-        while (*(volatile unsigned*)arrive < (unsigned)M) {
-            if (++spins > kPairSpinLimit) {
-                atomicExch(err, 2);
-                res = -1;
-                break;
+        int res = 0;
+        if (skip) {
+            res = -1;
+        } else {
+            if (fail)
+                atomicAdd(fails, 1u);
+            __threadfence();
+            atomicAdd(arrive, 1u);
+            int spins = 0;
+            while (*(volatile unsigned*)arrive < (unsigned)M) {
+                if (++spins > limit) {
+                    atomicExch(err, 2);
+                    res = -1;
+                    break;
+                }
+                __nanosleep(200);
             }
-            __nanosleep(200);
+            __threadfence();
+            if (res == 0)
+                res = *(volatile unsigned*)fails == 0 ? 1 : 0;
         }
-        __threadfence();
-        if (res == 0)
-            res = *(volatile unsigned*)fails == 0 ? 1 : 0;
         s_res = res;
     }
     __syncthreads();
@@ -761,7 +827,9 @@ __global__ void __launch_bounds__(384, PM ? 2 : 1) k_decode_pair(DecodeParams p)
                 const int fail = syndrome_pair<PO>(c, fr, &s_flag, s_row);
                 if (t == 0)
                     s_flag = 0; /* read again only after later barriers */
-                const int v = pair_team_vote(sync + 2 * it, M, fail != 0, p.err);
+                const int v = pair_team_vote(sync + 2 * it, M, fail != 0, p.err,
+                                             p.wait_limit > 0 ? p.wait_limit : kDefaultWaitLimit,
+                                             (int)blockIdx.x + 1 == p.skip_vote);
                 ok = v == 1;
                 if (v < 0 || ok || it >= p.max_iter)
                     break;

@@ -175,7 +175,7 @@ drx_ldpc_mix* drx_ldpc_mix_new(int ncodes, const drx_fec_params* params, const c
     std::vector<const DevCode*> ptrs;
     for (auto* h : m->codes)
         ptrs.push_back(h->dcode);
-    bool ok = cuda_check(cudaMalloc(&m->d_codes, sizeof(DevCode*) * ncodes), "cudaMalloc") &&
+    bool ok = cuda_check(drxg::dev_malloc(&m->d_codes, sizeof(DevCode*) * ncodes), "cudaMalloc") &&
               cuda_check(cudaMemcpy(m->d_codes, ptrs.data(), sizeof(DevCode*) * ncodes, cudaMemcpyHostToDevice),
                          "cudaMemcpy") &&
               cuda_check(cudaStreamCreateWithFlags(&m->capture, cudaStreamNonBlocking), "cudaStreamCreate") &&
@@ -317,10 +317,10 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
         m->dclass_max);
     const int mix_grid = std::min(nframes, m->mix_ctas * m->sms);
     total = std::max(total, mix_slab * (size_t)mix_grid);
-    if (!cuda_check(cudaMalloc(&m->d_frame_code, sizeof(int32_t) * nframes), "cudaMalloc") ||
-        !cuda_check(cudaMalloc(&m->d_order, sizeof(int32_t) * nframes), "cudaMalloc") ||
-        !cuda_check(cudaMalloc(&m->d_work, sizeof(unsigned) * (2 * ncodes + 1)), "cudaMalloc") ||
-        !cuda_check(cudaMalloc(&m->d_msg, total), "cudaMalloc") ||
+    if (!cuda_check(drxg::dev_malloc(&m->d_frame_code, sizeof(int32_t) * nframes), "cudaMalloc") ||
+        !cuda_check(drxg::dev_malloc(&m->d_order, sizeof(int32_t) * nframes), "cudaMalloc") ||
+        !cuda_check(drxg::dev_malloc(&m->d_work, sizeof(unsigned) * (2 * ncodes + 1)), "cudaMalloc") ||
+        !cuda_check(drxg::dev_malloc(&m->d_msg, total), "cudaMalloc") ||
         !cuda_check(cudaMemcpy(m->d_frame_code, code, sizeof(int32_t) * nframes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
         !cuda_check(cudaMemcpy(m->d_order, order.data(), sizeof(int32_t) * nframes, cudaMemcpyHostToDevice), "cudaMemcpy")) {
         release_plan(m);
@@ -338,11 +338,11 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
                 li[c] = h->learn_iters;
             }
         }
-        if (!cuda_check(cudaMalloc(&m->d_learn, sizeof(void*) * ncodes), "cudaMalloc") ||
-            !cuda_check(cudaMalloc(&m->d_learn_cls, sizeof(void*) * ncodes), "cudaMalloc") ||
-            !cuda_check(cudaMalloc(&m->d_learn_iters, sizeof(int) * ncodes), "cudaMalloc") ||
-            !cuda_check(cudaMalloc(&m->d_fb_rows, sizeof(int32_t) * (nframes + 4 + ncodes)), "cudaMalloc") ||
-            !cuda_check(cudaMalloc(&m->d_fb_ok, nframes), "cudaMalloc") ||
+        if (!cuda_check(drxg::dev_malloc(&m->d_learn, sizeof(void*) * ncodes), "cudaMalloc") ||
+            !cuda_check(drxg::dev_malloc(&m->d_learn_cls, sizeof(void*) * ncodes), "cudaMalloc") ||
+            !cuda_check(drxg::dev_malloc(&m->d_learn_iters, sizeof(int) * ncodes), "cudaMalloc") ||
+            !cuda_check(drxg::dev_malloc(&m->d_fb_rows, sizeof(int32_t) * (nframes + 4 + ncodes)), "cudaMalloc") ||
+            !cuda_check(drxg::dev_malloc(&m->d_fb_ok, nframes), "cudaMalloc") ||
             !cuda_check(cudaMemcpy(m->d_learn, lt.data(), sizeof(void*) * ncodes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
             !cuda_check(cudaMemcpy(m->d_learn_cls, lc.data(), sizeof(void*) * ncodes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
             !cuda_check(cudaMemcpy(m->d_learn_iters, li.data(), sizeof(int) * ncodes, cudaMemcpyHostToDevice), "cudaMemcpy")) {

@@ -154,6 +154,27 @@ int drx_channel_generate(drx_ldpc* d, const char* constellation, const char* con
 #define DRX_VARIANT_PAIR 2
 int drx_ldpc_set_variant(drx_ldpc* d, int variant);
 
+/* New: how long a group barrier of this handle's group-stopping launches
+ * (drx_ldpc_decode, and stop > 0) waits for the other CTAs of its team, in
+ * polls about 200 ns apart; 0 restores the default (4,194,304 polls, about
+ * a second).  A barrier that gives up ends its group's decode with the
+ * frames flagged as failed and sets the device error word to 2
+ * (drx_ldpc_device_error).  Returns 0, or -1. */
+int drx_ldpc_set_wait_limit(drx_ldpc* d, int polls);
+
+/* Testing hook: in this handle's later group-stopping launches, CTA `cta`
+ * never arrives at its team's barriers, so that the other members' waits
+ * run out (the time-out path of the group barrier); -1 turns it off.
+ * Returns 0, or -1. */
+int drx_ldpc_test_skip_vote(drx_ldpc* d, int cta);
+
+/* Testing hook: after `after` more device allocations by this library (all
+ * threads), the next one fails as an out-of-memory cudaMalloc would, once;
+ * -1 turns it off.  The failing call reports the error as every other
+ * allocation failure does (NULL from drx_ldpc_new, -1 from a decode call,
+ * drx_ldpc_last_error()). */
+void drx_test_fail_device_alloc(int after);
+
 /* ---- mixed batches: several codes (MODCODs, normal and short) at once ---- */
 
 typedef struct drx_ldpc_mix drx_ldpc_mix;
@@ -307,6 +328,63 @@ int drx_bch_decode_device(drx_bch* b, uint8_t* cw, size_t stride, int32_t* resul
  * benchmark frames): encode nframes device rows in place, the kbch message
  * bits of each row followed by its nbch - kbch parity bits.  Asynchronous. */
 int drx_bch_encode_device(drx_bch* b, uint8_t* cw, size_t stride, int nframes, void* stream);
+
+/* ---- the receiver's FEC stage on the GPU ---- */
+
+/* New: the FEC chain on device rows, on one stream: LDPC decode of nframes
+ * frames into cw (kldpc bits, MSB first, frame f at cw + f * cw_stride;
+ * iters and ok as drx_ldpc_decode_device), then BCH decode of every
+ * codeword in place, bch_result[f] = corrected bits or -1.  The BCH decode
+ * runs whatever the LDPC outcome, as the reference's receivers do: the
+ * DVB-T2 FEC path (libdvbrx/src/dvbt2.c:2386-2396, drx_ldpc_decode on
+ * batches of drx_ldpc_lanes() blocks, so stop = 64 reproduces it, then
+ * drx_bch_decode per block) and the DVB-S2 output thread
+ * (libdvbrx/src/rxmt.c:547-552).  b must be the BCH code of d's FEC
+ * parameters.  Asynchronous on `stream` (NULL: d's stream).  Returns 0 if
+ * the work was queued. */
+int drx_fec_decode_device(drx_ldpc* d, drx_bch* b, const int8_t* llr, size_t llr_stride, uint8_t* cw,
+                          size_t cw_stride, int32_t* iters, uint8_t* ok, int32_t* bch_result, int nframes,
+                          int max_iter, int stop, void* stream);
+
+/* New: a receiver's frame queue in front of the GPU, replacing the LDPC
+ * worker pool and output ordering of the reference's multi-threaded
+ * receiver (libdvbrx/src/rxmt.c:214-275, 476-480, 514-536, 570-606).
+ * Frames are pushed one at a time with the index of their code (codes
+ * given at creation: params[c], rates[c]).  Each code has at most one open
+ * batch and at most max_open batches are open (a frame of another code
+ * sends the oldest, as batch_for does); a batch is sent when it holds
+ * batch_frames frames, when it has been open longer than max_latency_ms
+ * (0: no bound), on drx_rxq_flush, or when drx_rxq_pop waits for one of
+ * its frames.  A sent batch is decoded on the GPU on its code's stream
+ * (copy in, drx_fec_decode_device, copy out); stop 0 stops each frame on
+ * its own, stop 1 decodes the batch as one group (the reference's
+ * drx_ldpc_decode on the batch).  Batches of different codes overlap on the
+ * GPU.  Frames leave in arrival order (sequence numbers 0, 1, 2, ...). */
+typedef struct drx_rxq drx_rxq;
+drx_rxq* drx_rxq_new(int ncodes, const drx_fec_params* params, const char* const* rates, int batch_frames,
+                     int max_open, int max_iter, int stop, int max_latency_ms);
+void drx_rxq_free(drx_rxq* q);
+
+/* Queue frame llr (host, nldpc int8 of code `code`); *fseq (may be NULL)
+ * receives its sequence number.  The LLRs are copied before the call
+ * returns.  Returns 0, or -1. */
+int drx_rxq_push(drx_rxq* q, int code, const int8_t* llr, uint64_t* fseq);
+
+/* Send every open batch.  Returns 0, or -1. */
+int drx_rxq_flush(drx_rxq* q);
+
+/* The next frame in arrival order, if its batch is done (wait = 0), or
+ * after sending its batch if needed and waiting for it (wait = 1): its
+ * sequence number and code, ceil(kldpc/8) bytes of BCH-corrected codeword
+ * into cw (the first kbch bits are the BBFRAME), the LDPC iterations and
+ * syndrome flag (the batch's, with stop 1) and the BCH result (corrected
+ * bits or -1).  Any output pointer may be NULL.  Returns 1 if a frame was
+ * returned, 0 if none is ready or the queue is empty, -1 on error. */
+int drx_rxq_pop(drx_rxq* q, int wait, uint64_t* fseq, int* code, uint8_t* cw, int32_t* iters, int32_t* ok,
+                int32_t* bch_result);
+
+/* Frames pushed and not yet popped (-1 for NULL). */
+int drx_rxq_pending(const drx_rxq* q);
 
 /* ---- soft demapper (reference libdvbrx/src/demap.c:491-533) -------------
  *

@@ -359,8 +359,11 @@ def run_mix(args, world, rank, learned=False):
         errs += int((out[rows, : h.nbytes] != info[rows, : h.nbytes]).any(dim=1).sum())
     res = {"value": aggregate_gbps(world, 1, bits, ms), "unit": UNIT, "frames_per_rank": n, "codes": len(codes),
            "normal_share": float(np.mean([s == 0 for s, _, _, _ in spec])), "ms_per_batch": ms,
-           "tiling": {D.TILING_ONE_LAUNCH: "one launch", D.TILING_PER_CODE: "per code"}[choice],
-           "tune_ms": {"one_launch": t_one, "per_code": t_per}, "fer": errs / n,
+           "tiling": {D.TILING_ONE_LAUNCH: "one launch, one frame per CTA", D.TILING_PER_CODE: "per code",
+                      D.TILING_ONE_LAUNCH_PAIR: "one launch, two frames per CTA"}[choice],
+           "tune_ms": {"one_launch_one_frame_per_cta": t_one, "per_code": t_per,
+                       "one_launch_two_frames_per_cta": mix.tuned_ms(D.TILING_ONE_LAUNCH_PAIR)},
+           "fer": errs / n,
            "avg_iterations": float(it.float().mean()),
            "esn0": "QEF (EN 302 307-1 Table 13, normal-frame values for both sizes) + 0.5 dB",
            "max_iter": MAX_ITER}

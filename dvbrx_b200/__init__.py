@@ -101,6 +101,8 @@ def lib():
         L.drx_ldpc_mix_set_tiling.restype = ip
         L.drx_ldpc_mix_tune.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         L.drx_ldpc_mix_tune.restype = ip
+        L.drx_ldpc_mix_tuned_ms.argtypes = [vp, ip]
+        L.drx_ldpc_mix_tuned_ms.restype = ctypes.c_float
         L.drx_ldpc_mix_run.argtypes = [vp, vp]
         L.drx_ldpc_mix_run.restype = ip
         L.drx_ldpc_set_variant.argtypes = [vp, ip]
@@ -497,7 +499,7 @@ class Bch:
         return result
 
 
-TILING_ONE_LAUNCH, TILING_PER_CODE = 1, 2  # DRX_TILING_*
+TILING_ONE_LAUNCH, TILING_PER_CODE, TILING_ONE_LAUNCH_PAIR = 1, 2, 3  # DRX_TILING_*
 
 
 class LdpcMix:
@@ -580,9 +582,15 @@ class LdpcMix:
         if self._lib.drx_ldpc_mix_set_tiling(self.h, int(tiling)) < 0:
             raise ValueError(last_error())
 
+    def tuned_ms(self, tiling):
+        """``drx_ldpc_mix_tuned_ms``: the tuner's time of a tiling (None if the
+        plan lacks it)."""
+        v = self._lib.drx_ldpc_mix_tuned_ms(self.h, int(tiling))
+        return None if v < 0 else v
+
     def tune(self, stream=None):
-        """Times both tilings on the planned batch; returns (choice,
-        ms_one_launch, ms_per_code)."""
+        """Times every tiling of the plan on the planned batch; returns
+        (choice, ms_one_launch, ms_per_code); tuned_ms gives the rest."""
         import torch
         s = stream if stream is not None else torch.cuda.current_stream()
         a, b = ctypes.c_float(), ctypes.c_float()

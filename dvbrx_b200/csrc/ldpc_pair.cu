@@ -81,6 +81,19 @@ size_t decode_pair_msg_bytes(int R, int kid)
     return rec + (k.pm == 2 ? a16h(sizeof(uint16_t) * (size_t)(R - kQCp)) : 0);
 }
 
+bool pair_kernel_shape(int kid, int* a, int* b, int* gdm, int* ls, int* pm)
+{
+    if (kid < 0 || kid >= (int)kernels().size())
+        return false;
+    const PairKernel& k = kernels()[kid];
+    *a = k.a;
+    *b = k.b;
+    *gdm = k.gdm;
+    *ls = k.ls;
+    *pm = k.pm;
+    return true;
+}
+
 /* the twin of a mode-0 kernel in mode pm (1 or 2), -1 if it has none */
 int pair_kernel_twin(int kid, int pm)
 {

@@ -776,6 +776,95 @@ static __device__ int pair_team_vote(unsigned* slot, int M, bool fail, int* err,
     return r;
 }
 
+/* Lane state of a frame-pair CTA (shared memory): the frame and iteration
+ * of each lane, the syndrome flags, the lanes to reload, the syndrome
+ * scan's start rows. */
+struct PairLanes {
+    int frame[2], iter[2], flag, reload, row[2];
+};
+
+/* Per-frame stopping: frames stream through the two lanes independently.
+ * A lane whose frame passes the syndrome check or reaches max_iter writes
+ * its results and takes the next frame of the batch (the counter p.work;
+ * work item k is row p.rows[k], or k), so a converged frame never waits for
+ * its neighbour.  The CTA's tables are staged (fr) and its lane state
+ * initialised (frames -1, both lanes to reload, flag 0, rows 0). */
+template <int A, int B, int GDM, int LS, bool PO>
+__device__ __forceinline__ void stream_frames(const DecodeParams& p, const DevCode& c, const PairFrame& fr, void* msg,
+                                              int lT, int nframes, PairLanes& st)
+{
+    int* s_frame = st.frame;
+    int* s_iter = st.iter;
+    int& s_flag = st.flag;
+    int& s_reload = st.reload;
+    int* s_row = st.row;
+    const int t = threadIdx.x;
+    uint32_t fresh = 0;
+    for (;;) {
+        /* lanes that need a frame take the next one of the batch */
+        const int reload = s_reload;
+        if (reload) {
+            if (t == 0) {
+                for (int h = 0; h < 2; h++)
+                    if (reload & (1 << h)) {
+                        const int f = (int)atomicAdd(p.work, 1u);
+                        s_frame[h] = f < nframes ? f : -1;
+                        s_iter[h] = 0;
+                    }
+            }
+            __syncthreads();
+            for (int h = 0; h < 2; h++)
+                if (reload & (1 << h)) {
+                    const int f = s_frame[h];
+                    const int row = f < 0 ? 0 : p.rows ? p.rows[f] : f;
+                    load_lane<PO>(c, fr, f >= 0 ? p.llr + (size_t)row * p.llr_stride : nullptr, h);
+                    fresh |= 0xFFFFu << (16 * h);
+                }
+            if (t == 0)
+                s_reload = 0;
+            __syncthreads();
+        }
+        if (s_frame[0] < 0 && s_frame[1] < 0)
+            break;
+        const int fail = syndrome_pair<PO>(c, fr, &s_flag, s_row);
+        /* lanes whose frame is done: results out, refill */
+        int done = 0;
+        for (int h = 0; h < 2; h++) {
+            const int f = s_frame[h];
+            if (f >= 0 && (!((fail >> h) & 1) || s_iter[h] >= p.max_iter)) {
+                const int row = p.rows ? p.rows[f] : f;
+                store_lane(c, fr, h, p.out + (size_t)row * p.out_stride);
+                if (t == 0) {
+                    if (p.iters)
+                        p.iters[row] = s_iter[h];
+                    if (p.ok)
+                        p.ok[row] = (fail >> h) & 1 ? 0 : 1;
+                }
+                done |= 1 << h;
+            }
+        }
+        __syncthreads();
+        if (t == 0) {
+            s_flag = 0;
+            s_reload = done;
+        }
+        __syncthreads();
+        if (done)
+            continue; /* reload, then check the new frames first */
+        if (lT)
+            iterate_pair<A, B, GDM, LS, true, PO>(c, fr, msg, fresh, learn_row(s_iter[0], lT),
+                                                  learn_row(s_iter[1], lT));
+        else
+            iterate_pair<A, B, GDM, LS, false, PO>(c, fr, msg, fresh, -1, -1);
+        fresh = 0;
+        if (t == 0) {
+            s_iter[0]++;
+            s_iter[1]++;
+        }
+        __syncthreads();
+    }
+}
+
 /* PM: 0 one resident CTA per SM; 1 two (80 registers), for codes whose
  * posteriors leave room for two (short frames); 2 two, with the parity
  * posteriors out of shared memory (PO: normal frames up to rate 4/5) */
@@ -784,7 +873,11 @@ __global__ void __launch_bounds__(384, PM ? 2 : 1) k_decode_pair(DecodeParams p)
 {
     constexpr bool PO = PM == 2;
     extern __shared__ __align__(16) char smem[];
-    __shared__ int s_frame[2], s_iter[2], s_flag, s_reload, s_row[2];
+    __shared__ int s_lanes[sizeof(PairLanes) / sizeof(int)];
+    int* s_frame = ((PairLanes*)s_lanes)->frame;
+    int& s_flag = ((PairLanes*)s_lanes)->flag;
+    int& s_reload = ((PairLanes*)s_lanes)->reload;
+    int* s_row = ((PairLanes*)s_lanes)->row;
     const DevCode c = *p.code;
     constexpr bool WIDE = (GDM > 0 ? GDM : B + 2) > 16;
     void* msg = (char*)p.msg + (size_t)blockIdx.x * p.msg_stride;
@@ -852,70 +945,8 @@ __global__ void __launch_bounds__(384, PM ? 2 : 1) k_decode_pair(DecodeParams p)
         }
         return;
     }
-    uint32_t fresh = 0;
-    for (;;) {
-        /* lanes that need a frame take the next one of the batch */
-        const int reload = s_reload;
-        if (reload) {
-            if (t == 0) {
-                for (int h = 0; h < 2; h++)
-                    if (reload & (1 << h)) {
-                        const int f = (int)atomicAdd(p.work, 1u);
-                        s_frame[h] = f < nframes ? f : -1;
-                        s_iter[h] = 0;
-                    }
-            }
-            __syncthreads();
-            for (int h = 0; h < 2; h++)
-                if (reload & (1 << h)) {
-                    const int f = s_frame[h];
-                    const int row = f < 0 ? 0 : p.rows ? p.rows[f] : f;
-                    load_lane<PO>(c, fr, f >= 0 ? p.llr + (size_t)row * p.llr_stride : nullptr, h);
-                    fresh |= 0xFFFFu << (16 * h);
-                }
-            if (t == 0)
-                s_reload = 0;
-            __syncthreads();
-        }
-        if (s_frame[0] < 0 && s_frame[1] < 0)
-            break;
-        const int fail = syndrome_pair<PO>(c, fr, &s_flag, s_row);
-        /* lanes whose frame is done: results out, refill */
-        int done = 0;
-        for (int h = 0; h < 2; h++) {
-            const int f = s_frame[h];
-            if (f >= 0 && (!((fail >> h) & 1) || s_iter[h] >= p.max_iter)) {
-                const int row = p.rows ? p.rows[f] : f;
-                store_lane(c, fr, h, p.out + (size_t)row * p.out_stride);
-                if (t == 0) {
-                    if (p.iters)
-                        p.iters[row] = s_iter[h];
-                    if (p.ok)
-                        p.ok[row] = (fail >> h) & 1 ? 0 : 1;
-                }
-                done |= 1 << h;
-            }
-        }
-        __syncthreads();
-        if (t == 0) {
-            s_flag = 0;
-            s_reload = done;
-        }
-        __syncthreads();
-        if (done)
-            continue; /* reload, then check the new frames first */
-        if (lT)
-            iterate_pair<A, B, GDM, LS, true, PO>(c, fr, msg, fresh, learn_row(s_iter[0], lT),
-                                                  learn_row(s_iter[1], lT));
-        else
-            iterate_pair<A, B, GDM, LS, false, PO>(c, fr, msg, fresh, -1, -1);
-        fresh = 0;
-        if (t == 0) {
-            s_iter[0]++;
-            s_iter[1]++;
-        }
-        __syncthreads();
-    }
+    PairLanes& st = *(PairLanes*)s_lanes;
+    stream_frames<A, B, GDM, LS, PO>(p, c, fr, msg, lT, nframes, st);
 }
 
 /* Pair kernels by information-link counts (A, B): every pair of the DVB-S2,

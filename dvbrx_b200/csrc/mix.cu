@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "handle.h"
+#include "mixpair.h"
 
 using namespace drxg;
 
@@ -61,9 +62,13 @@ struct drx_ldpc_mix {
     int* d_learn_iters = nullptr;
     int32_t* d_fb_rows = nullptr;
     uint8_t* d_fb_ok = nullptr;
-    cudaGraphExec_t exec[3] = {};
+    /* one launch, two frames per CTA: per code start, count, shape, weight,
+     * then the first code of every CTA; one counter per code */
+    int* d_pair = nullptr;
+    unsigned* d_pair_work = nullptr;
+    cudaGraphExec_t exec[4] = {};
     int tiling = DRX_TILING_ONE_LAUNCH;
-    float tuned_ms[3] = {};
+    float tuned_ms[4] = {};
 };
 
 namespace {
@@ -84,6 +89,10 @@ void release_plan(drx_ldpc_mix* m)
     cudaFree(m->d_learn_iters);
     cudaFree(m->d_fb_rows);
     cudaFree(m->d_fb_ok);
+    cudaFree(m->d_pair);
+    cudaFree(m->d_pair_work);
+    m->d_pair = nullptr;
+    m->d_pair_work = nullptr;
     m->d_learn = nullptr;
     m->d_learn_cls = nullptr;
     m->d_learn_iters = nullptr;
@@ -317,12 +326,68 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
         m->dclass_max);
     const int mix_grid = std::min(nframes, m->mix_ctas * m->sms);
     total = std::max(total, mix_slab * (size_t)mix_grid);
+
+    /* one launch, two frames per CTA (plain plans, every code of the batch
+     * with a shape in the mixed kernel): shared memory and slab of the
+     * largest code, CTAs spread over the codes by their work */
+    bool pair_plan = !learned;
+    std::vector<int> shape(ncodes, -1), weight(ncodes, 0);
+    size_t pair_smem = 0, pair_slab = 0;
+    for (int c = 0; c < ncodes && pair_plan; c++) {
+        if (!count[c])
+            continue;
+        drx_ldpc* h = m->codes[c];
+        const int kid = pair_runs(h) ? pair_kernel_id(h->code) : -1;
+        int a, b, g, ls, pm;
+        if (kid < 0 || !pair_kernel_shape(kid, &a, &b, &g, &ls, &pm) || (shape[c] = mix_pair_shape(a, b, g, ls)) < 0) {
+            pair_plan = false;
+            break;
+        }
+        weight[c] = (int)std::min<long long>(h->code.edges, 1 << 30);
+        pair_smem = std::max(pair_smem, decode_pair_smem_bytes(h->code.N, h->code.K, (int)h->code.ent.size() / 2,
+                                                               (int)h->code.steps.size(), h->code.q, kid));
+        pair_slab = std::max(pair_slab, decode_pair_msg_bytes(h->code.R, kid));
+    }
+    int pair_grid = 0;
+    std::vector<int> pair_host;
+    if (pair_plan) {
+        pair_grid = std::min(decode_mix_pair_ctas_per_sm(pair_smem) * m->sms, (nframes + 1) / 2);
+        pair_plan = pair_grid > 0;
+    }
+    if (pair_plan) {
+        pair_host.assign(4 * (size_t)ncodes + pair_grid, 0);
+        double wsum = 0;
+        for (int c = 0; c < ncodes; c++) {
+            pair_host[c] = start[c];
+            pair_host[ncodes + c] = count[c];
+            pair_host[2 * ncodes + c] = shape[c];
+            pair_host[3 * ncodes + c] = weight[c];
+            wsum += (double)count[c] * weight[c];
+        }
+        /* CTA k starts on the code whose share of the work covers (k + 1/2) / grid */
+        double acc = 0;
+        int ci = 0;
+        for (int k = 0; k < pair_grid; k++) {
+            const double at = (k + 0.5) / pair_grid * wsum;
+            while (ci < ncodes && acc + (double)count[corder[ci]] * weight[corder[ci]] < at) {
+                acc += (double)count[corder[ci]] * weight[corder[ci]];
+                ci++;
+            }
+            pair_host[4 * (size_t)ncodes + k] = corder[std::min(ci, ncodes - 1)];
+        }
+        total = std::max(total, pair_slab * (size_t)pair_grid);
+    }
     if (!cuda_check(drxg::dev_malloc(&m->d_frame_code, sizeof(int32_t) * nframes), "cudaMalloc") ||
         !cuda_check(drxg::dev_malloc(&m->d_order, sizeof(int32_t) * nframes), "cudaMalloc") ||
         !cuda_check(drxg::dev_malloc(&m->d_work, sizeof(unsigned) * (2 * ncodes + 1)), "cudaMalloc") ||
         !cuda_check(drxg::dev_malloc(&m->d_msg, total), "cudaMalloc") ||
         !cuda_check(cudaMemcpy(m->d_frame_code, code, sizeof(int32_t) * nframes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
-        !cuda_check(cudaMemcpy(m->d_order, order.data(), sizeof(int32_t) * nframes, cudaMemcpyHostToDevice), "cudaMemcpy")) {
+        !cuda_check(cudaMemcpy(m->d_order, order.data(), sizeof(int32_t) * nframes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
+        (pair_plan &&
+         (!cuda_check(drxg::dev_malloc(&m->d_pair, sizeof(int) * pair_host.size()), "cudaMalloc") ||
+          !cuda_check(drxg::dev_malloc(&m->d_pair_work, sizeof(unsigned) * ncodes), "cudaMalloc") ||
+          !cuda_check(cudaMemcpy(m->d_pair, pair_host.data(), sizeof(int) * pair_host.size(), cudaMemcpyHostToDevice),
+                      "cudaMemcpy")))) {
         release_plan(m);
         return -1;
     }
@@ -355,13 +420,17 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
     m->nframes = nframes;
     /* kernel attributes are set before capture (not a stream operation) */
     decode_mix_ctas_per_sm(m->dclass_max, m->mix_smem);
+    if (pair_plan)
+        decode_mix_pair_ctas_per_sm(pair_smem);
     for (auto* h : m->codes) {
         decode_ctas_per_sm(h->code.dclass, h->smem);
         if (h->pair_ctas_per_sm > 0)
             decode_pair_ctas_per_sm(h->pair_kid, h->pair_smem);
     }
 
-    for (int t = DRX_TILING_ONE_LAUNCH; t <= DRX_TILING_PER_CODE; t++) {
+    for (int t = DRX_TILING_ONE_LAUNCH; t <= DRX_TILING_ONE_LAUNCH_PAIR; t++) {
+        if (t == DRX_TILING_ONE_LAUNCH_PAIR && !pair_plan)
+            continue;
         cudaGraph_t g = nullptr;
         if (!cuda_check(cudaStreamBeginCapture(m->capture, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture")) {
             release_plan(m);
@@ -392,6 +461,31 @@ int plan_mix(drx_ldpc_mix* m, int nframes, const int32_t* code, const int8_t* ll
             e = cudaMemsetAsync(p.work, 0, sizeof(unsigned), m->capture);
             if (e == cudaSuccess)
                 e = launch_decode_mix(p, m->dclass_max, m->mix_smem, mix_grid, m->capture);
+        } else if (t == DRX_TILING_ONE_LAUNCH_PAIR) {
+            MixPairParams p{};
+            p.base.codes = m->d_codes;
+            p.base.frame_code = m->d_frame_code;
+            p.base.order = m->d_order;
+            p.base.llr = llr;
+            p.base.llr_stride = llr_stride;
+            p.base.out = out;
+            p.base.out_stride = out_stride;
+            p.base.iters = iters;
+            p.base.ok = ok;
+            p.base.nframes = nframes;
+            p.base.max_iter = max_iter;
+            p.base.msg = m->d_msg;
+            p.base.msg_stride = pair_slab;
+            p.code_start = m->d_pair;
+            p.code_count = m->d_pair + ncodes;
+            p.code_shape = m->d_pair + 2 * ncodes;
+            p.code_weight = m->d_pair + 3 * ncodes;
+            p.cta_code = m->d_pair + 4 * ncodes;
+            p.code_work = m->d_pair_work;
+            p.ncodes = ncodes;
+            e = cudaMemsetAsync(m->d_pair_work, 0, sizeof(unsigned) * ncodes, m->capture);
+            if (e == cudaSuccess)
+                e = launch_decode_mix_pair(p, pair_smem, pair_grid, m->capture);
         } else {
             e = cudaEventRecord(m->fork, m->capture);
             for (int s = 0; s < kSideStreams && e == cudaSuccess; s++)
@@ -529,8 +623,13 @@ int drx_ldpc_mix_set_learned(drx_ldpc_mix* m, int code_index, int iters, int ncl
 
 int drx_ldpc_mix_set_tiling(drx_ldpc_mix* m, int tiling)
 {
-    if (!m || (tiling != DRX_TILING_ONE_LAUNCH && tiling != DRX_TILING_PER_CODE)) {
+    if (!m || tiling < DRX_TILING_ONE_LAUNCH || tiling > DRX_TILING_ONE_LAUNCH_PAIR) {
         set_error("drx_ldpc_mix_set_tiling: unknown tiling");
+        return -1;
+    }
+    if (m->nframes && !m->exec[tiling]) {
+        set_error("drx_ldpc_mix_set_tiling: the plan has no such tiling (two frames per CTA in one launch needs "
+                  "a plain plan of DVB-S2 codes)");
         return -1;
     }
     m->tiling = tiling;
@@ -559,7 +658,10 @@ int drx_ldpc_mix_tune(drx_ldpc_mix* m, void* stream, float* ms_one_launch, float
     cudaEventCreate(&b);
     float best = 0;
     int choice = DRX_TILING_ONE_LAUNCH;
-    for (int t = DRX_TILING_ONE_LAUNCH; t <= DRX_TILING_PER_CODE; t++) {
+    for (int t = DRX_TILING_ONE_LAUNCH; t <= DRX_TILING_ONE_LAUNCH_PAIR; t++) {
+        m->tuned_ms[t] = 0;
+        if (!m->exec[t])
+            continue;
         float tmin = 1e30f;
         cudaGraphLaunch(m->exec[t], s); /* warm-up */
         for (int r = 0; r < 2; r++) {
@@ -589,6 +691,13 @@ int drx_ldpc_mix_tune(drx_ldpc_mix* m, void* stream, float* ms_one_launch, float
         *ms_per_code = m->tuned_ms[DRX_TILING_PER_CODE];
     m->tiling = choice;
     return choice;
+}
+
+float drx_ldpc_mix_tuned_ms(const drx_ldpc_mix* m, int tiling)
+{
+    if (!m || tiling < DRX_TILING_ONE_LAUNCH || tiling > DRX_TILING_ONE_LAUNCH_PAIR)
+        return -1.0f;
+    return m->exec[tiling] ? m->tuned_ms[tiling] : -1.0f;
 }
 
 }  // extern "C"

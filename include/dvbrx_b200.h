@@ -211,17 +211,26 @@ int drx_ldpc_mix_plan_learned(drx_ldpc_mix* m, int nframes, const int32_t* code,
                               uint8_t* fallback, int learned_iters, int plain_max_iter);
 
 /* Tilings of a mixed batch (identical results): one persistent launch over
- * all frames, one frame per CTA; or one persistent launch per code with the
+ * all frames, one frame per CTA; one persistent launch per code with the
  * code's own kernel (two frames per CTA where the frame-pair kernel
- * applies) on concurrent graph branches. */
+ * applies) on concurrent graph branches; or one persistent launch over all
+ * frames with two frames per CTA, each CTA running one code at a time with
+ * that code's frame-pair kernel shape and moving to the code with the most
+ * work left when its code runs out (plain plans whose codes are DVB-S2
+ * codes).  drx_ldpc_mix_set_tiling returns -1 for a tiling the plan lacks. */
 #define DRX_TILING_ONE_LAUNCH 1
 #define DRX_TILING_PER_CODE 2
+#define DRX_TILING_ONE_LAUNCH_PAIR 3
 int drx_ldpc_mix_set_tiling(drx_ldpc_mix* m, int tiling);
 
-/* Autotuner: decodes the planned batch with each tiling (twice, after a
- * warm-up), keeps the faster and returns it; the times in ms if non-NULL.
- * Synchronous. */
+/* Autotuner: decodes the planned batch with each tiling the plan has
+ * (twice, after a warm-up), keeps the fastest and returns it; the times of
+ * the first two tilings in ms if non-NULL (drx_ldpc_mix_tuned_ms gives
+ * every tiling's).  Synchronous. */
 int drx_ldpc_mix_tune(drx_ldpc_mix* m, void* stream, float* ms_one_launch, float* ms_per_code);
+
+/* The autotuner's time of a tiling in ms, -1 if the plan lacks it. */
+float drx_ldpc_mix_tuned_ms(const drx_ldpc_mix* m, int tiling);
 
 /* Launch the plan's graph (the tuned or set tiling) on `stream`. */
 int drx_ldpc_mix_run(drx_ldpc_mix* m, void* stream);

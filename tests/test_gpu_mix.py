@@ -77,6 +77,10 @@ def test_mixed_batch_tilings_and_tuner():
         mix.set_tiling(tiling)
         mix.run()
         check()
+    # S2X codes have no shape in the two-frames-per-CTA one-launch kernel: the plan lacks that tiling
+    with pytest.raises(ValueError):
+        mix.set_tiling(D.TILING_ONE_LAUNCH_PAIR)
+    assert mix.tuned_ms(D.TILING_ONE_LAUNCH_PAIR) is None
     choice, t1, t2 = mix.tune()
     assert choice in (D.TILING_ONE_LAUNCH, D.TILING_PER_CODE) and t1 > 0 and t2 > 0
     out.zero_()
@@ -143,3 +147,54 @@ def test_mixed_batch_learned_with_fallback():
             assert (got_i[rows] == i).all(), (CODES[c], tiling)
             assert (got_o[rows] == o).all(), (CODES[c], tiling)
             assert (got_f[rows] == f).all(), (CODES[c], tiling)
+
+
+# DVB-S2 codes of every shape of the two-frames-per-CTA one-launch kernel
+S2_CODES = [(0, r, "QPSK", es) for r, es in (("1_4", -1.9), ("1_3", -0.9), ("2_5", -0.1), ("1_2", 1.2),
+                                               ("3_5", 2.4), ("2_3", 3.3), ("3_4", 4.2), ("4_5", 4.8),
+                                               ("5_6", 5.3), ("8_9", 6.5), ("9_10", 6.8))] + \
+           [(1, r, "QPSK", es) for r, es in (("1_4", -1.2), ("1_2", 1.8), ("3_5", 2.9), ("2_3", 3.8),
+                                               ("3_4", 4.6), ("5_6", 5.8), ("8_9", 6.9))]
+
+
+def test_mixed_batch_one_launch_two_frames_per_cta():
+    """The one-launch tiling with two frames per CTA (CTAs taking one code at
+    a time, moving to the code with the most work left) gives the per-code
+    results exactly, and the tuner times all three tilings."""
+    import torch
+    n = 900
+    rng = np.random.default_rng(11)
+    code = rng.integers(0, len(S2_CODES), size=n).astype(np.int32)
+    llr = torch.zeros((n, 64800), dtype=torch.int8, device="cuda")
+    for c, (short, rate, const, es) in enumerate(S2_CODES):
+        rows = np.nonzero(code == c)[0]
+        if len(rows):
+            h = D.Ldpc(D.fec_lookup(short, rate), rate)
+            l, _, _ = h.generate(len(rows), es, seed=700 + c, constellation=const)
+            llr[torch.from_numpy(rows).cuda().long(), : h.N] = l
+            h.close()
+    mix = D.LdpcMix([(s, r) for s, r, _, _ in S2_CODES])
+    res = {}
+    out = torch.zeros((n, 7290), dtype=torch.uint8, device="cuda")
+    it = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    ok = torch.full((n,), 9, dtype=torch.uint8, device="cuda")
+    mix.plan(code, llr, out, it, ok, 30)
+    for tiling in (D.TILING_PER_CODE, D.TILING_ONE_LAUNCH_PAIR, D.TILING_ONE_LAUNCH):
+        out.zero_()
+        it.fill_(-1)
+        ok.fill_(9)
+        mix.set_tiling(tiling)
+        mix.run()
+        torch.cuda.synchronize()
+        res[tiling] = (out.cpu().numpy(), it.cpu().numpy(), ok.cpu().numpy())
+    for a, b in zip(res[D.TILING_PER_CODE], res[D.TILING_ONE_LAUNCH_PAIR]):
+        assert np.array_equal(a, b)
+    for a, b in zip(res[D.TILING_PER_CODE], res[D.TILING_ONE_LAUNCH]):
+        assert np.array_equal(a, b)
+    its = res[D.TILING_PER_CODE][1]
+    assert its.min() < its.max() and 0 < res[D.TILING_PER_CODE][2].sum() < n, "uneven iterations expected"
+    choice, t1, t2 = mix.tune()
+    t3 = mix.tuned_ms(D.TILING_ONE_LAUNCH_PAIR)
+    assert t1 > 0 and t2 > 0 and t3 is not None and t3 > 0
+    assert choice in (D.TILING_ONE_LAUNCH, D.TILING_PER_CODE, D.TILING_ONE_LAUNCH_PAIR)
+    mix.close()

@@ -115,6 +115,69 @@ def minibatch(dec, n, es_lo, es_hi, constellation, rng, chunks=8):
     return torch.cat(llrs), torch.cat(infos)
 
 
+def int8_minibatch(dec, n, es_lo, es_hi, constellation, rng, chunks=8, decodable_iters=0, max_draws=6):
+    """n frames in `chunks` groups, each at an Es/N0 drawn uniformly in
+    [es_lo, es_hi], as the int8 decoder receives them (the quantised int8
+    LLRs, carried in FP16 exactly): (FP16 LLRs [n, N], packed information
+    bits).  With the int8 inputs, the float model at scale 1 and offset 1 is
+    the plain int8 decoder frame for frame.  decodable_iters > 0 keeps only
+    the frames the plain int8 decoder decodes correctly within that many
+    iterations (the loss then rewards reaching the right answer sooner, not
+    lower confidence on frames no decoder recovers); the draw is repeated
+    until n frames are kept (at most max_draws times, the kept frames then
+    repeated to fill the batch)."""
+    sizes = [n // chunks + (1 if k < n % chunks else 0) for k in range(chunks)]
+    llrs, infos, have = [], [], 0
+    for _ in range(max_draws):
+        for s in sizes:
+            if s == 0:
+                continue
+            es = float(rng.uniform(es_lo, es_hi))
+            llr, info, _ = dec.generate(s, es, seed=int(rng.integers(1, 2**62)), constellation=constellation,
+                                        info=True)
+            if decodable_iters > 0:
+                bits, _, _ = dec.decode_device(llr, decodable_iters)
+                good = (bits == info).all(dim=1)
+                llr, info = llr[good], info[good]
+            llrs.append(llr)
+            infos.append(info)
+            have += llr.shape[0]
+        if have >= n:
+            break
+    llr, info = torch.cat(llrs), torch.cat(infos)
+    if llr.shape[0] == 0:
+        raise RuntimeError("no decodable frame in the Es/N0 range")
+    if llr.shape[0] < n:
+        idx = torch.arange(n, device=llr.device) % llr.shape[0]
+        llr, info = llr[idx], info[idx]
+    return llr[:n].to(torch.float16), info[:n]
+
+
+def int8_selection_set(dec, es_points, n, constellation, seed=4321):
+    """Fixed frames for model selection: int8 LLRs and information bits per
+    Es/N0 point."""
+    out = []
+    for k, es in enumerate(es_points):
+        llr, info, _ = dec.generate(n, float(es), seed=seed + k, constellation=constellation, info=True)
+        out.append((float(es), llr, info))
+    return out
+
+
+def int8_fer(dec, beta, alpha, cod, sset, iters):
+    """FER of the int8 learned decoder (the table rounded to Q8 as the library
+    does, no fallback) on a selection set, and its mean iterations."""
+    dec.set_learned(beta.detach().float().cpu().numpy(), alpha.detach().float().cpu().numpy(), cod)
+    errs = frames = 0
+    its = 0.0
+    for _, llr, info in sset:
+        bits, it, _, _ = dec.decode_learned(llr, iters, 0)
+        errs += int((bits != info).any(dim=1).sum())
+        frames += llr.shape[0]
+        its += float(it.float().sum())
+    dec.set_learned(None, None, None)
+    return errs / frames, its / frames
+
+
 def loss_weights(kind, iters):
     """Per-iteration weights of the BCE sums: "uniform", "ramp" ((t + 1) / T)
     or "last" (the final iteration only)."""
@@ -154,9 +217,15 @@ def validate(model, vset):
 
 
 def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, lr, seed, log=None,
-          weights="uniform", val_points=None):
+          weights="uniform", val_points=None, int8_inputs=False, decodable_iters=0, select_points=None,
+          select_frames=1024, eval_every=20):
     """Adam on the fp32 masters of the FP16 tables, initialised to the
-    plain decoder (scale 1, offset 1).  Returns (model, history)."""
+    plain decoder (scale 1, offset 1).  int8_inputs / decodable_iters: the
+    minibatches of int8_minibatch.  select_points: Es/N0 points of a fixed
+    selection set; every eval_every steps the int8 learned decoder's FER at
+    `iters` iterations is measured there, and the model keeps the best tables
+    seen (the plain decoder's to start with), so that the result is never
+    worse than the plain decoder on that set.  Returns (model, history)."""
     world, rank = dist_world()
     torch.manual_seed(seed)
     rng = np.random.default_rng(rank_seed(seed, rank))
@@ -167,9 +236,21 @@ def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, l
         log(json.dumps({"validation_init": validate(model, vset)}))
     opt = torch.optim.Adam(model.parameters(), lr=lr)
     hist = []
+    sset = int8_selection_set(model.dec, select_points, select_frames, constellation) if select_points else None
+    best = None
+    if sset:
+        f0, i0 = int8_fer(model.dec, model.beta, model.alpha, model.cod, sset, iters)
+        best = (f0, i0, model.beta.detach().clone(), model.alpha.detach().clone(), -1)
+        model.selection = {"plain_fer": f0, "plain_avg_iters": i0}
+        if log:
+            log(json.dumps({"selection_plain": {"fer": f0, "avg_iters": i0}}))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for k in range(steps):
-        llr16, info = minibatch(model.dec, batch, es_lo, es_hi, constellation, rng)
+        if int8_inputs or decodable_iters:
+            llr16, info = int8_minibatch(model.dec, batch, es_lo, es_hi, constellation, rng,
+                                         decodable_iters=decodable_iters)
+        else:
+            llr16, info = minibatch(model.dec, batch, es_lo, es_hi, constellation, rng)
         torch.cuda.synchronize()
         ev0.record()
         loss = model(llr16, info)
@@ -182,9 +263,22 @@ def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, l
         ev1.record()
         torch.cuda.synchronize()
         rec = {"step": k, "loss": float(loss.detach()), "ms": ev0.elapsed_time(ev1)}
+        if sset and ((k + 1) % eval_every == 0 or k == steps - 1):
+            f, i = int8_fer(model.dec, model.beta, model.alpha, model.cod, sset, iters)
+            rec.update({"select_fer": f, "select_avg_iters": i})
+            if (f, i) < (best[0], best[1]):
+                best = (f, i, model.beta.detach().clone(), model.alpha.detach().clone(), k)
         hist.append(rec)
         if log and (k % 10 == 0 or k == steps - 1):
             log(json.dumps(rec))
+    if best is not None:
+        with torch.no_grad():
+            model.beta.copy_(best[2])
+            model.alpha.copy_(best[3])
+        model.selection.update({"fer": best[0], "avg_iters": best[1], "step": best[4],
+                                "points": list(select_points), "frames_per_point": select_frames})
+        if log:
+            log(json.dumps({"selection_best": model.selection}))
     model.validation = validate(model, vset)
     if log:
         log(json.dumps({"validation_final": model.validation}))
@@ -263,6 +357,13 @@ def main(argv=None):
     ap.add_argument("--plain-iters", type=int, default=30)
     ap.add_argument("--weights", default="uniform", choices=["uniform", "ramp", "last"])
     ap.add_argument("--val", type=float, nargs="*", default=None, help="validation Es/N0 points")
+    ap.add_argument("--int8-inputs", action="store_true",
+                    help="train on the int8 LLRs the decoder receives (carried in FP16)")
+    ap.add_argument("--decodable", type=int, default=0,
+                    help="keep only frames the plain int8 decoder decodes within this many iterations")
+    ap.add_argument("--select", type=float, nargs="*", default=None,
+                    help="Es/N0 points of the model-selection set (int8 FER at --iters iterations)")
+    ap.add_argument("--select-frames", type=int, default=1024)
     ap.add_argument("--all-s2", action="store_true",
                     help="one table per DVB-S2 code (normal and short), trained on the rate's QPSK MODCOD over "
                          "[QEF - 0.25, QEF + 0.75] dB, into --out-dir")
@@ -317,12 +418,14 @@ def main(argv=None):
         return 0
     t0 = time.time()
     model, hist = train(a.short, a.rate, a.const, a.iters, a.batch, a.es[0], a.es[1], a.steps, a.lr, a.seed, log,
-                        a.weights, a.val)
+                        a.weights, a.val, int8_inputs=a.int8_inputs, decodable_iters=a.decodable,
+                        select_points=a.select, select_frames=a.select_frames)
     wall = time.time() - t0
     ms = [h["ms"] for h in hist[1:]] or [hist[0]["ms"]]
     meta = {"short": a.short, "rate": a.rate, "constellation": a.const, "es": a.es, "batch": a.batch,
             "steps": a.steps, "lr": a.lr, "seed": a.seed, "weights": a.weights,
-            "validation": model.validation,
+            "validation": model.validation, "int8_inputs": a.int8_inputs, "decodable_iters": a.decodable,
+            "selection": getattr(model, "selection", None),
             "loss_first": hist[0]["loss"], "loss_last": float(np.mean([h["loss"] for h in hist[-10:]])),
             "train_ms_per_step": float(np.median(ms)), "train_frames_per_s": a.batch / (float(np.median(ms)) * 1e-3),
             "train_wall_s": wall}

@@ -322,11 +322,12 @@ struct PairCheck {
             m1 = __viaddmax_s16x2(c1, 0xFFFFFFFFu, 0u);
         }
         if (take) {
-            const uint32_t sm = lmask(sg);
-            a0 = sel(sm, neg2(m0), m0);
-            a1 = sel(sm, neg2(m1), m1);
-            b0 = neg2(a0);
-            b1 = neg2(a1);
+            /* both signs of each candidate side by side (the level steps wait on this chain) */
+            const uint32_t sm = lmask(sg), q0 = neg2(m0), q1 = neg2(m1);
+            a0 = sel(sm, q0, m0);
+            a1 = sel(sm, q1, m1);
+            b0 = sel(sm, m0, q0);
+            b1 = sel(sm, m1, q1);
             nidx = (min0 & 0x001F001Fu) | 0x64006400u; /* FP16 1024 + slot of min0 */
             /* per lane min0 (6 bits) | min1 << 6, magnitudes capped at 32 (| index << 12 below degree 17) */
             recw = __vmins2(m0, 0x00200020u) | (__vmins2(m1, 0x00200020u) << 6);

@@ -134,3 +134,28 @@ def test_trained_table_gains_over_plain():
         assert fer_learned <= 0.5 * fer_plain, (es, fer_learned, fer_plain)
         assert float(li.float().mean()) < float(pi.float().mean()), es
         assert int(((fb_bits != info).any(dim=1)).sum()) <= int(((full != info).any(dim=1)).sum()), es
+
+
+def test_config4_table_beats_plain_at_equal_iterations():
+    """The committed config-4 table (normal 2/3 8PSK, 20 unrolled
+    iterations, trained on the GPU with the project's forward and backward
+    kernels over Es/N0 6.0-7.5 dB) against the plain decoder at the same
+    20-iteration budget on the same frames: in the waterfall it at least
+    halves the frame error rate and needs fewer iterations."""
+    from dvbrx_b200 import train
+
+    table = train.load_table(0, "2_3", "8PSK", 20)
+    assert table is not None and table["iters"] == 20
+    dec = D.Ldpc(D.fec_lookup(0, "2_3"), "2_3")
+    train.apply_table(dec, table)
+    for es in (6.6, 6.65):
+        llr, info, _ = dec.generate(2048, es, seed=9090, constellation="8PSK", info=True)
+        pb, pi, _ = dec.decode_device(llr, 20)
+        lb, li, _, _ = dec.decode_learned(llr, 20, 0)
+        torch.cuda.synchronize()
+        fer_plain = float((pb != info).any(dim=1).float().mean())
+        fer_learned = float((lb != info).any(dim=1).float().mean())
+        assert fer_plain > 0.02, (es, fer_plain)
+        assert fer_learned <= 0.5 * fer_plain, (es, fer_learned, fer_plain)
+        assert float(li.float().mean()) < float(pi.float().mean()), es
+    dec.close()

@@ -32,10 +32,14 @@ namespace drxg {
     X(6, 9, 9, 0, 2) X(7, 12, 12, 0, 2) X(8, 9, 9, 0, 3) X(9, 16, 16, 0, 4) X(10, 20, 20, 0, 3)          \
     X(11, 25, 25, 0, 6) X(12, 28, 28, 0, 4) X(13, 1, 1, 7, 3) X(14, 1, 1, 14, 3) X(15, 1, 1, 22, 5)
 
+/* One code's frames with its shape: its tables staged in the shape's form,
+ * then the streaming loop of the frame-pair kernel. */
 template <int A, int B, int GDM, int LS>
-__device__ __noinline__ void mix_code_frames(const DecodeParams& p, const DevCode& c, const PairFrame& fr, void* msg,
+__device__ __noinline__ void mix_code_frames(const DecodeParams& p, const DevCode& c, char* smem, void* msg,
                                              PairLanes& st)
 {
+    const PairFrame fr = stage_pair<false, pair_key_form(A, B, GDM, LS)>(c, smem, nullptr);
+    __syncthreads();
     stream_frames<A, B, GDM, LS, false>(p, c, fr, msg, 0, p.nframes, st);
 }
 
@@ -68,7 +72,6 @@ __global__ void __launch_bounds__(384, 1) k_decode_mix_pair(MixPairParams mp)
     __syncthreads();
     for (int code = s_code; code >= 0;) {
         const DevCode c = *mp.base.codes[code];
-        const PairFrame fr = stage_pair<false>(c, smem, nullptr);
         if (t == 0) {
             st.frame[0] = st.frame[1] = -1;
             st.flag = 0;
@@ -91,7 +94,7 @@ __global__ void __launch_bounds__(384, 1) k_decode_mix_pair(MixPairParams mp)
         switch (mp.code_shape[code]) {
 #define DRXG_MIX_CASE(k, a, b, g, ls)                    \
     case k:                                              \
-        mix_code_frames<a, b, g, ls>(p, c, fr, msg, st); \
+        mix_code_frames<a, b, g, ls>(p, c, smem, msg, st); \
         break;
             DRXG_MIX_SHAPES(DRXG_MIX_CASE)
 #undef DRXG_MIX_CASE

@@ -143,9 +143,10 @@ __device__ __forceinline__ uint32_t sign_mask(uint32_t w, int k)
  * PO: the parity posteriors (slots 0 and 1) are not in shared memory; the
  * layer loop hands their two-byte words in and takes the new ones back. */
 template <int DM, bool EXACT, int LS, bool WIDE, bool PO>
-struct PairCheck {
+struct PairCheckKey {
     static_assert(DM <= (WIDE ? 32 : 16), "degree above the record's slots");
     using Rec = PairRec<WIDE>;
+    static constexpr bool kKeys = true;
     static constexpr int S = DM;
     /* slots that can be late or early: K0 .. K1 (link slots 2 .. 2 LS + 1) */
     static constexpr int K0 = 2;
@@ -397,6 +398,252 @@ struct PairCheck {
     }
 };
 
+/*
+ * The previous form of the check node (min form), kept for the kernels where
+ * it measures faster (low check degrees, and levelled codes whose wavefront
+ * steps wait on the check's finish): minimums over |x| itself, the index of
+ * min0 found in the write pass (|x| > min0 per slot), sign bits of slot k
+ * at bit k (lane A) and 16 + k (lane B), entries as (shared byte address of
+ * the link for check 0 before the wrap, a).  Both forms give the reference's
+ * results; a kernel uses one form throughout (its records, entries and
+ * syndrome scan).
+ */
+template <int DM, bool EXACT, int LS, bool WIDE, bool PO>
+struct PairCheckMin {
+    static_assert(DM <= (WIDE ? 32 : 16), "degree above the record's slots");
+    using Rec = PairRec<WIDE>;
+    static constexpr bool kKeys = false;
+    static constexpr int S = DM;
+    /* slots that can be late or early: K0 .. K1 (link slots 2 .. 2 LS + 1) */
+    static constexpr int K0 = 2;
+    static constexpr int K1 = S - 1 < 2 * LS + 1 ? S - 1 : 2 * LS + 1;
+    uint32_t addr[S]; /* shared-memory byte addresses of the owned links' posteriors */
+    uint32_t x[S];
+    uint32_t live, inm, outm; /* bit k: slot k is a link / is read late / is written early */
+    uint32_t n0, n1, p0, p1, idxh, sgn, sgn1; /* sgn: sign bits of slots 0-15, sgn1: 16-31 */
+    uint32_t min0, min1, sg, mn0, mn1;
+    uint32_t m0p1, nmn0, nmn1; /* min0 + 1, -mn0, -mn1 (set by finish) */
+
+    __device__ __forceinline__ void setup(const int2* __restrict__ ent, int cnt, int K, int q, int i, int j,
+                                          Rec rec, uint32_t fresh, unsigned long long meta, uint32_t sbase)
+    {
+        const int D = EXACT ? DM : cnt + 2;
+        const int pc = K + kQCp * i + j;
+        const int pp = i ? pc - kQCp : K + kQCp * (q - 1) + j - 1;
+        uint32_t lv = (1u << D) - 1u;
+        if ((i | j) == 0)
+            lv &= ~2u;
+        live = lv;
+        inm = (uint32_t)(meta >> 8) & 0xFFFFFFu;
+        outm = (uint32_t)(meta >> 32) & 0xFFFFFFu;
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            if (k < 2) {
+                addr[k] = PO ? 0u : sbase + 2u * (uint32_t)(k == 0 ? pc : pp);
+            } else {
+                /* a slot past the degree takes the last link's address: read, never used */
+                const int2 e = ent[min(k, D - 1) - 2];
+                addr[k] = (uint32_t)e.x + 2u * (uint32_t)j + (j < e.y ? 2u * kQCp : 0u);
+            }
+        }
+        /* messages: zero for a lane in its first iteration */
+        const uint32_t w0 = rec.x & ~fresh;
+        sgn = rec.y & ~fresh;
+        const uint32_t m0 = w0 & 0x003F003Fu, m1 = (w0 >> 6) & 0x003F003Fu;
+        if constexpr (WIDE) {
+            sgn1 = rec.z & ~fresh;
+            idxh = (rec.w & ~fresh) | 0x64006400u; /* FP16 1024 + index */
+        } else {
+            sgn1 = 0;
+            idxh = ((w0 >> 12) & 0x000F000Fu) | 0x64006400u; /* FP16 1024 + index */
+        }
+        /* minus the message: +m if it is negative, else -min(m, 31) */
+        n0 = m0;
+        n1 = m1;
+        p0 = __viaddmax_s16x2(~m0, 0x00010001u, 0xFFE1FFE1u); /* max(-m, -31) */
+        p1 = __viaddmax_s16x2(~m1, 0x00010001u, 0xFFE1FFE1u);
+        min0 = min1 = 0x00FF00FFu;
+        sg = 0;
+    }
+
+    /* minus the old message of slot k */
+    __device__ __forceinline__ uint32_t unmsg(int k) const
+    {
+        const uint32_t im = heq(idxh, 0x64006400u + (uint32_t)k * 0x00010001u);
+        const uint32_t sm = lmask((k < 16 ? sgn : sgn1) << (15 - (k & 15)));
+        return sel(sm, sel(im, n1, n0), sel(im, p1, p0));
+    }
+
+    __device__ __forceinline__ void fold(uint32_t v)
+    {
+        const uint32_t a = abs2(v);
+        min1 = __vmins2(min1, __vmaxs2(min0, a));
+        min0 = __vmins2(min0, a);
+        sg ^= v;
+    }
+
+    /* every slot but the late ones, without branches; minimums folded
+     * two slots at a time: min1 = second smallest of {min0, min1, a, b} =
+     * min3(max(min0, min(a, b)), min1, max(a, b)).  LEV: the layer has late
+     * slots; otherwise only the slots that can be absent are masked (the
+     * previous parity of check (0, 0)). */
+    template <bool LEV>
+    __device__ __forceinline__ void read_all(const uint16_t* __restrict__ post, uint32_t r0, uint32_t r1)
+    {
+        const uint32_t excl = LEV ? (~live | inm) : ~live;
+        uint32_t f[S];
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            const uint32_t m = unmsg(k);
+            const uint32_t raw = PO && k < 2 ? (k == 0 ? r0 : r1) : lds16(addr[k]);
+            uint32_t v = sadd(sx2(raw), m);
+            if (LEV || !EXACT || k == 1)
+                v = ((excl >> k) & 1u) ? 0x00FF00FFu : v;
+            f[k] = v;
+            /* a late slot keeps minus its old message for read_late */
+            x[k] = LEV && ((inm >> k) & 1u) ? m : v;
+        }
+#pragma unroll
+        for (int k = 0; k + 1 < S; k += 2) {
+            const uint32_t a = abs2(f[k]), b = abs2(f[k + 1]);
+            const uint32_t lo = __vmins2(a, b), hi = __vmaxs2(a, b);
+            min1 = __vimin3_s16x2(__vmaxs2(min0, lo), min1, hi);
+            min0 = __vimin3_s16x2(min0, a, b);
+            sg ^= f[k] ^ f[k + 1];
+        }
+        if (S & 1)
+            fold(f[S - 1]);
+    }
+
+    /* a thread that holds no check (t >= 360): valid addresses, no links, so
+     * that it can run the warp-uniform level steps of its warp */
+    __device__ __forceinline__ void idle(uint32_t sbase)
+    {
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            addr[k] = sbase;
+            x[k] = 0x00FF00FFu;
+        }
+        live = inm = outm = 0;
+        n0 = n1 = p0 = p1 = sgn = sgn1 = 0;
+        idxh = 0x64006400u;
+        min0 = min1 = 0x00FF00FFu;
+        sg = mn0 = mn1 = m0p1 = nmn0 = nmn1 = 0;
+    }
+
+    /* the late slots (their bits were written by earlier levels) of a check
+     * in the current level (mine); other threads keep their state.  Shared
+     * links come first in every layer (codes.cpp), so late and early slots
+     * are among slots 2 .. KE */
+    template <int KE>
+    __device__ __forceinline__ void read_late(const uint16_t* __restrict__ post, bool mine)
+    {
+        const uint32_t im = mine ? inm : 0u;
+#pragma unroll
+        for (int k = K0; k <= KE; k++) {
+            const bool in = (im >> k) & 1u;
+            const uint32_t v = sadd(sx2(lds16(addr[k])), x[k]);
+            x[k] = in ? v : x[k];
+            fold(in ? v : 0x00FF00FFu);
+        }
+    }
+
+    /* the cap at 127 and offset 1, or the learned scale and offset of each
+     * lane's iteration (lpA, lpB).  Only threads with `take` keep the result:
+     * the level steps run it on whole warps */
+    __device__ __forceinline__ void finish(bool take, bool learned, uint32_t lpA, uint32_t lpB)
+    {
+        const uint32_t c1 = min1, c0 = min0;
+        uint32_t m0, m1;
+        if (learned) {
+            const uint32_t k0 = __vmins2(c0, 0x007F007Fu), k1 = __vmins2(c1, 0x007F007Fu);
+            m0 = (uint32_t)learned_mag(k0 & 0xFFFF, lpA) | (uint32_t)learned_mag(k0 >> 16, lpB) << 16;
+            m1 = (uint32_t)learned_mag(k1 & 0xFFFF, lpA) | (uint32_t)learned_mag(k1 >> 16, lpB) << 16;
+        } else {
+            m0 = __viaddmax_s16x2(__vmins2(c0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+            m1 = __viaddmax_s16x2(__vmins2(c1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
+        }
+        if (take) {
+            mn0 = m0;
+            mn1 = m1;
+            m0p1 = __vadd2(c0, 0x00010001u);
+            nmn0 = neg2(m0);
+            nmn1 = neg2(m1);
+        }
+    }
+
+    /* new posterior of slot k (two bytes), and its masks: lanes where
+     * |x| is above min0 (the slot does not hold the minimum) and lanes whose
+     * outgoing message is negative */
+    __device__ __forceinline__ uint32_t update(int k, uint32_t& above, uint32_t& neg) const
+    {
+        const uint32_t v = x[k];
+        /* min0 - |x| = min(min0 + x, (min0 + 1) + ~x) < 0 */
+        above = lmask(__viaddmin_s16x2(~v, m0p1, __vadd2(min0, v)));
+        neg = lmask(sg ^ v);
+        const uint32_t o = sel(neg, sel(above, nmn0, nmn1), sel(above, mn0, mn1));
+        return pk2(sadd(v, o));
+    }
+
+    /* posteriors that later levels of the layer read (checks of the current
+     * level only) */
+    template <int KE>
+    __device__ __forceinline__ void write_early(uint16_t* __restrict__ post, bool mine) const
+    {
+        const uint32_t om = mine ? outm : 0u;
+#pragma unroll
+        for (int k = K0; k <= KE; k++) {
+            uint32_t above, neg;
+            const uint32_t nv = update(k, above, neg);
+            if ((om >> k) & 1u)
+                sts16(addr[k], nv);
+        }
+    }
+
+    /* every other posterior (predicated stores) and the node's compressed
+     * messages for both lanes, stored by thread 0: the slot holding min0 and
+     * one sign bit per slot.  PO: the parity words go to o0 and o1. */
+    __device__ __forceinline__ void write_rest(uint16_t* __restrict__ post, Rec* __restrict__ dst, uint32_t& o0,
+                                               uint32_t& o1)
+    {
+        const uint32_t wm = live & ~outm;
+        uint32_t nidx = 0, nsg = 0, nsg1 = 0; /* nidx per lane: k + 1 of a slot holding min0, 0 if none */
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            uint32_t above, neg;
+            const uint32_t nv = update(k, above, neg);
+            if (PO && k < 2)
+                (k == 0 ? o0 : o1) = nv;
+            else if ((wm >> k) & 1u)
+                sts16(addr[k], nv);
+            nidx = sel(above, nidx, (uint32_t)(k + 1) * 0x00010001u);
+            if (k < 16)
+                nsg |= neg & (0x00010001u << k);
+            else
+                nsg1 |= neg & (0x00010001u << (k - 16));
+        }
+        nidx = __viaddmax_s16x2(nidx, 0xFFFFFFFFu, 0u); /* slot number: max(nidx - 1, 0) */
+        const uint32_t m0c = __vmins2(mn0, 0x00200020u), m1c = __vmins2(mn1, 0x00200020u);
+        if constexpr (WIDE)
+            __stcg(dst, make_uint4(m0c | (m1c << 6), nsg, nsg1, nidx));
+        else
+            __stcg(dst, make_uint2(m0c | (m1c << 6) | (nidx << 12), nsg));
+    }
+};
+
+
+/* The form a kernel uses: the key form where it measured faster (normal
+ * 1/2 and 3/5, whose layers have 5 and 9 information links and one pair of
+ * shared links, and check degrees 22 and above), the min form elsewhere. */
+__host__ __device__ constexpr bool pair_key_form(int a, int b, int gdm, int ls)
+{
+    return gdm == 0 && ((a == b && (a == 5 || a == 9) && ls == 2) || a >= 20);
+}
+
+template <int DM, bool EXACT, int LS, bool WIDE, bool PO, bool KEYS>
+using PairCheck = typename std::conditional<KEYS, PairCheckKey<DM, EXACT, LS, WIDE, PO>,
+                                            PairCheckMin<DM, EXACT, LS, WIDE, PO>>::type;
+
 struct PairFrame {
     uint16_t* post;
     const int2* ent; /* (shared byte address of the link group's first word, -2 a) */
@@ -411,7 +658,7 @@ struct PairFrame {
 
 __device__ __forceinline__ size_t a16p(size_t v) { return (v + 15) & ~(size_t)15; }
 
-template <bool PO>
+template <bool PO, bool KEYS>
 __device__ PairFrame stage_pair(const DevCode& c, char* smem, uint16_t* gpar)
 {
     PairFrame f;
@@ -428,13 +675,16 @@ __device__ PairFrame stage_pair(const DevCode& c, char* smem, uint16_t* gpar)
     uint16_t* eoff = (uint16_t*)(smem + off);
     off += a16p(sizeof(uint16_t) * (c.q + 1));
     uint32_t* steps = (uint32_t*)(smem + off);
-    /* entries (360 g - a, a) as (shared byte address of group g's first
-     * posterior word, -2 a): the link of check j is word (j - a) mod 360 of
-     * the group, at byte offset min(u, u + 720), u = 2 j - 2 a unsigned */
+    /* entries (360 g - a, a) as, in the key form, (shared byte address of
+     * group g's first posterior word, -2 a): the link of check j is word
+     * (j - a) mod 360 of the group, at byte offset min(u, u + 720),
+     * u = 2 j - 2 a unsigned; in the min form (shared byte address of the
+     * link of check 0 before the wrap, a): x + 2 j, + 720 if j < a */
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(f.post);
     for (int k = threadIdx.x; k < c.nent; k += blockDim.x) {
         const int2 e = c.ent[k];
-        ent[k] = make_int2((int)(sbase + 2u * (uint32_t)(e.x + e.y)), -2 * e.y);
+        ent[k] = KEYS ? make_int2((int)(sbase + 2u * (uint32_t)(e.x + e.y)), -2 * e.y)
+                      : make_int2((int)(sbase + 2u * (uint32_t)e.x), e.y);
     }
     for (int k = threadIdx.x; k <= c.q; k += blockDim.x)
         eoff[k] = c.eoff[k];
@@ -516,7 +766,7 @@ __device__ __forceinline__ void parity_words(const DevCode& c, const PairFrame& 
     }
 }
 
-template <bool PO>
+template <bool PO, bool KEYS>
 __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int* sflag, volatile int* srow)
 {
     const int t = threadIdx.x;
@@ -553,8 +803,14 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
                 const int e1 = fr.eoff[i + 1];
                 for (int e = fr.eoff[i]; e < e1; e++) {
                     const int2 en = fr.ent[e];
-                    const uint32_t u = 2u * (uint32_t)j + (uint32_t)en.y;
-                    const uint32_t v = sx2(lds16((uint32_t)en.x + __viaddmin_u32(u, 2u * kQCp, u)));
+                    uint32_t a;
+                    if (KEYS) {
+                        const uint32_t u = 2u * (uint32_t)j + (uint32_t)en.y;
+                        a = (uint32_t)en.x + __viaddmin_u32(u, 2u * kQCp, u);
+                    } else {
+                        a = (uint32_t)en.x + 2u * (uint32_t)j + (j < en.y ? 2u * kQCp : 0u);
+                    }
+                    const uint32_t v = sx2(lds16(a));
                     par ^= v;
                     z |= __vadd2(v, 0xFFFFFFFFu) & ~v;
                 }
@@ -586,7 +842,7 @@ __device__ int syndrome_pair(const DevCode& c, const PairFrame& fr, volatile int
  * constrain the bits two checks of a layer share, so the wavefront levels
  * carry just those links.  Unlevelled layers take one pass.
  */
-template <int DM, bool EXACT, int LS, bool WIDE, bool LEARNED, bool PO>
+template <int DM, bool EXACT, int LS, bool WIDE, bool LEARNED, bool PO, bool KEYS>
 __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c, int i, int cnt, int nlev,
                                            PairRec<WIDE> rec, unsigned long long meta, uint32_t fresh,
                                            PairRec<WIDE>* __restrict__ msg, int lA, int lB, uint32_t r0,
@@ -604,7 +860,7 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
             b = s_learn_tab[lB + k];
         }
     };
-    using Ck = PairCheck<DM, EXACT, LS, WIDE, PO>;
+    using Ck = PairCheck<DM, EXACT, LS, WIDE, PO, KEYS>;
     Ck ck;
     if (active) {
         ck.setup(fr.ent + fr.eoff[i], cnt, c.K, c.q, i, j, rec, fresh, meta,
@@ -698,13 +954,13 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, 
         const int cnt = fr.eoff[i + 1] - fr.eoff[i];
         const int nlev = c.nlev[i];
         if (GDM > 0)
-            layer_pair<(GDM > 0 ? GDM : 2), false, LS, WIDE, LEARNED, PO>(fr, c, i, cnt, nlev, rec, meta, fresh, msg,
+            layer_pair<(GDM > 0 ? GDM : 2), false, LS, WIDE, LEARNED, PO, pair_key_form(A, B, GDM, LS)>(fr, c, i, cnt, nlev, rec, meta, fresh, msg,
                                                                            lA, lB, r0, r1, o0, o1);
         else if (A == B || cnt == A)
-            layer_pair<A + 2, true, LS, WIDE, LEARNED, PO>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB, r0, r1,
+            layer_pair<A + 2, true, LS, WIDE, LEARNED, PO, pair_key_form(A, B, GDM, LS)>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB, r0, r1,
                                                            o0, o1);
         else
-            layer_pair<B + 2, true, LS, WIDE, LEARNED, PO>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB, r0, r1,
+            layer_pair<B + 2, true, LS, WIDE, LEARNED, PO, pair_key_form(A, B, GDM, LS)>(fr, c, i, cnt, nlev, rec, meta, fresh, msg, lA, lB, r0, r1,
                                                            o0, o1);
         /* (i - 1, j) is final for this iteration; (i, j) goes to the next
          * layer, or, for the last layer, to the check (0, j + 1) */
@@ -827,7 +1083,7 @@ __device__ __forceinline__ void stream_frames(const DecodeParams& p, const DevCo
         }
         if (s_frame[0] < 0 && s_frame[1] < 0)
             break;
-        const int fail = syndrome_pair<PO>(c, fr, &s_flag, s_row);
+        const int fail = syndrome_pair<PO, pair_key_form(A, B, GDM, LS)>(c, fr, &s_flag, s_row);
         /* lanes whose frame is done: results out, refill */
         int done = 0;
         for (int h = 0; h < 2; h++) {
@@ -884,7 +1140,7 @@ __global__ void __launch_bounds__(384, PM ? 2 : 1) k_decode_pair(DecodeParams p)
     void* msg = (char*)p.msg + (size_t)blockIdx.x * p.msg_stride;
     /* the parity words follow the message records in this CTA's slab */
     uint16_t* gpar = (uint16_t*)((char*)msg + (((size_t)c.R * (WIDE ? 16 : 8) + 15) & ~(size_t)15));
-    const PairFrame fr = stage_pair<PO>(c, smem, gpar);
+    const PairFrame fr = stage_pair<PO, pair_key_form(A, B, GDM, LS)>(c, smem, gpar);
     const int lT = stage_learn(p.learn, p.learn_class, p.learn_iters);
     const int nframes = p.nframes_dev ? *p.nframes_dev : p.nframes;
     const int t = threadIdx.x;
@@ -918,7 +1174,7 @@ __global__ void __launch_bounds__(384, PM ? 2 : 1) k_decode_pair(DecodeParams p)
             int it = 0;
             bool ok = true;
             for (;;) {
-                const int fail = syndrome_pair<PO>(c, fr, &s_flag, s_row);
+                const int fail = syndrome_pair<PO, pair_key_form(A, B, GDM, LS)>(c, fr, &s_flag, s_row);
                 if (t == 0)
                     s_flag = 0; /* read again only after later barriers */
                 const int v = pair_team_vote(sync + 2 * it, M, fail != 0, p.err,

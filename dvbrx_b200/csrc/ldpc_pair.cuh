@@ -882,21 +882,20 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
         lwords(wa, wb);
         auto steps = [&](auto ke) {
             constexpr int KE = decltype(ke)::value;
-            /* the last level writes nothing that a later check of the layer
-             * reads (the last writer of a shared bit is its last reader, and
-             * writes it in write_rest), so it needs neither early writes nor
-             * a barrier before the write pass */
+            /* the last level writes nothing early (no later check of the
+             * layer reads its bits); its barrier stays: without it the write
+             * pass of the other warps takes issue slots from the last level's
+             * chain, and the layer runs longer (measured) */
             for (int l = 0; l < nlev; l++) {
-                const bool mine = lev == l, last = l + 1 == nlev;
+                const bool mine = lev == l;
                 if (__any_sync(0xFFFFFFFFu, mine)) {
                     if (l > 0)
                         ck.template read_late<KE>(fr.post, mine);
                     ck.finish(mine, LEARNED, wa, wb);
-                    if (!last)
+                    if (l + 1 < nlev)
                         ck.template write_early<KE>(fr.post, mine);
                 }
-                if (!last)
-                    __syncthreads();
+                __syncthreads();
             }
         };
         constexpr int KS = Ck::K1 > 3 ? 3 : Ck::K1;

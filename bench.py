@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned decoder's line items")
     ap.add_argument("--no-bch", action="store_true", help="skip the BCH line item")
     ap.add_argument("--no-group", action="store_true", help="skip the 64-frame group-stopping line item")
+    ap.add_argument("--no-dropin", action="store_true", help="skip the drop-in call line item")
+    ap.add_argument("--dropin-calls", type=int, default=16, help="64-frame calls per worker thread")
     ap.add_argument("--mix-frames", type=int, default=16384,
                     help="frames of the mixed-MODCOD batch (0: skip that line item)")
     ap.add_argument("--variant", default="auto", choices=["auto", "frame"],
@@ -373,6 +375,51 @@ def run_mix(args, world, rank, learned=False):
     return res
 
 
+def run_dropin(host_batches, threads, calls_per_thread, world):
+    """The reference's own call pattern on the GPU: `threads` host threads
+    (the reference receiver's LDPC workers, rxmt.c:514-536), each with its
+    own handle, each decoding `calls_per_thread` drx_ldpc_decode calls of 64
+    frames from host memory through per-frame pointer arrays (the drop-in
+    entry point, reference batch semantics); wall clock over all threads."""
+    import ctypes
+    import threading
+
+    import dvbrx_b200 as D
+
+    p = D.fec_lookup(SHORT, RATE)
+    pool = np.ascontiguousarray(np.concatenate(host_batches))
+    handles = [D.Ldpc(p, RATE) for _ in range(threads)]
+    nb = handles[0].nbytes
+    outs = [np.zeros((64, nb), np.uint8) for _ in range(threads)]
+    PtrArr = ctypes.c_void_p * 64
+
+    def calls(w, n):
+        out_ptrs = PtrArr(*[outs[w][k].ctypes.data for k in range(64)])
+        for c in range(n):
+            f0 = ((w * n + c) * 64) % (pool.shape[0] - 63)
+            in_ptrs = PtrArr(*[pool[f0 + k].ctypes.data for k in range(64)])
+            handles[w]._lib.drx_ldpc_decode(handles[w].h, in_ptrs, out_ptrs, 64, MAX_ITER)
+
+    def run(n):
+        ts = [threading.Thread(target=calls, args=(w, n)) for w in range(threads)]
+        t0 = time.perf_counter()
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0
+
+    run(2)  # warm-up: scratch, staging, streams
+    dt = max_over_ranks(run(calls_per_thread), world, "cuda")
+    for h in handles:
+        h.close()
+    frames = threads * calls_per_thread * 64
+    return {"value": aggregate_gbps(world, frames, p.kldpc, dt * 1e3), "unit": UNIT, "threads": threads,
+            "frames_per_call": 64, "calls": threads * calls_per_thread, "seconds": dt,
+            "api": "drx_ldpc_decode (host per-frame pointers, 64 frames per call, one handle per thread; "
+                   "the frames of one call stop together, as in the reference)"}
+
+
 def run_demap(nframes, world, hbm_peak, reps=5):
     """The soft demapper ahead of the decoder: nframes 8PSK PLFRAMEs of the
     workload's MODCOD (random received symbols; the kernel's work does not
@@ -629,6 +676,11 @@ def run_b200(args):
         }
         dec.set_learned(None, None, None)
 
+    # the drop-in call as the reference's workers make it: 16 threads, 64-frame calls, host memory
+    dropin = None
+    if not args.no_dropin:
+        dropin = run_dropin([l[:1024].cpu().numpy() for l in llr], 16, args.dropin_calls, world)
+
     # the BCH outer code behind the decoder, the demapper ahead of it
     bch = None if args.no_bch else run_bch(F, world)
     demap = None if args.no_bch else run_demap(F, world, hbm_peak)
@@ -691,6 +743,7 @@ def run_b200(args):
             "decoder": "plain layered offset min-sum (bit-exact to the reference)",
             "quality": {"fer": fer, "avg_iterations": iters_sum / frames_rank},
             "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "group64": group64,
+            "dropin": dropin,
             "learned": learned,
             "mixed_modcod": mix_res, "mixed_modcod_learned": mix_learned, "bch": bch, "demapper": demap,
             "gpu_launches": args.steps,

@@ -882,18 +882,18 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
         lwords(wa, wb);
         auto steps = [&](auto ke) {
             constexpr int KE = decltype(ke)::value;
-            /* the last level writes nothing early (no later check of the
-             * layer reads its bits); its barrier stays: without it the write
-             * pass of the other warps takes issue slots from the last level's
-             * chain, and the layer runs longer (measured) */
+            /* every level ends with a CTA barrier, the last one too: without
+             * it the write pass of the other warps takes issue slots from the
+             * last level's chain and the layer runs longer (measured), and
+             * skipping the last level's early writes (it has none to store)
+             * measured slower as well */
             for (int l = 0; l < nlev; l++) {
                 const bool mine = lev == l;
                 if (__any_sync(0xFFFFFFFFu, mine)) {
                     if (l > 0)
                         ck.template read_late<KE>(fr.post, mine);
                     ck.finish(mine, LEARNED, wa, wb);
-                    if (l + 1 < nlev)
-                        ck.template write_early<KE>(fr.post, mine);
+                    ck.template write_early<KE>(fr.post, mine);
                 }
                 __syncthreads();
             }

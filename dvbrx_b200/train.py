@@ -364,6 +364,8 @@ def main(argv=None):
     ap.add_argument("--select", type=float, nargs="*", default=None,
                     help="Es/N0 points of the model-selection set (int8 FER at --iters iterations)")
     ap.add_argument("--select-frames", type=int, default=1024)
+    ap.add_argument("--select-offsets", type=float, nargs="*", default=None,
+                    help="--all-s2: selection points as offsets (dB) from each rate's QEF Es/N0")
     ap.add_argument("--all-s2", action="store_true",
                     help="one table per DVB-S2 code (normal and short), trained on the rate's QPSK MODCOD over "
                          "[QEF - 0.25, QEF + 0.75] dB, into --out-dir")
@@ -387,12 +389,17 @@ def main(argv=None):
                 q = qef_db("QPSK", rate)
                 es = [q - 0.25, q + 0.75]
                 t0 = time.time()
+                # selection (with --select-offsets): the int8 learned FER at QEF + each offset
+                sel = [q + o for o in a.select_offsets] if a.select_offsets else None
                 model, hist = train(short, rate, "QPSK", a.iters, a.batch, es[0], es[1], a.steps, a.lr, a.seed,
-                                    None, a.weights, [q, q + 0.25, q + 0.5])
+                                    None, a.weights, [q, q + 0.25, q + 0.5], int8_inputs=a.int8_inputs,
+                                    decodable_iters=a.decodable, select_points=sel, select_frames=a.select_frames)
                 ms = [h["ms"] for h in hist[1:]] or [hist[0]["ms"]]
                 meta = {"short": short, "rate": rate, "constellation": "QPSK", "es": es, "batch": a.batch,
                         "steps": a.steps, "lr": a.lr, "seed": a.seed, "weights": a.weights,
-                        "validation": model.validation, "loss_first": hist[0]["loss"],
+                        "validation": model.validation, "int8_inputs": a.int8_inputs,
+                        "decodable_iters": a.decodable, "selection": getattr(model, "selection", None),
+                        "loss_first": hist[0]["loss"],
                         "loss_last": float(np.mean([h["loss"] for h in hist[-10:]])),
                         "train_ms_per_step": float(np.median(ms)),
                         "train_frames_per_s": a.batch / (float(np.median(ms)) * 1e-3),

@@ -153,6 +153,8 @@ bool send_batch(drx_rxq* q, RxBatch* b)
     const size_t n = (size_t)b->n, N = (size_t)c.N, nb = (size_t)c.nbytes;
     cudaStream_t s = c.stream;
     b->sent = true;
+    /* on a failure the batch's frames are still popped (in order), with whatever the
+     * failed step left; the push or pop that sent it returns -1 */
     return cuda_check(cudaMemcpyAsync(b->d_llr, b->h_llr, n * N, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync") &&
            drx_fec_decode_device(c.ldpc, c.bch, b->d_llr, N, b->d_cw, nb, b->d_it, b->d_ok, b->d_bch, b->n,
                                  q->max_iter, q->stop ? b->n : 0, s) == 0 &&

@@ -368,7 +368,8 @@ int drx_fec_decode_device(drx_ldpc* d, drx_bch* b, const int8_t* llr, size_t llr
  * (copy in, drx_fec_decode_device, copy out); stop 0 stops each frame on
  * its own, stop 1 decodes the batch as one group (the reference's
  * drx_ldpc_decode on the batch).  Batches of different codes overlap on the
- * GPU.  Frames leave in arrival order (sequence numbers 0, 1, 2, ...). */
+ * GPU.  Frames leave in arrival order (sequence numbers 0, 1, 2, ...).  Like
+ * a decoder handle, a queue is used from one host thread at a time. */
 typedef struct drx_rxq drx_rxq;
 drx_rxq* drx_rxq_new(int ncodes, const drx_fec_params* params, const char* const* rates, int batch_frames,
                      int max_open, int max_iter, int stop, int max_latency_ms);

@@ -194,6 +194,11 @@ drx_rxq* drx_rxq_new(int ncodes, const drx_fec_params* params, const char* const
         set_error("drx_rxq_new: bad arguments");
         return nullptr;
     }
+    if (stop == 1 && batch_frames > drx_ldpc_lanes()) {
+        /* a group's CTAs wait for each other: the reference's batch of at most lanes frames */
+        set_error("drx_rxq_new: group decoding takes batches of at most drx_ldpc_lanes() frames");
+        return nullptr;
+    }
     drx_rxq* q = new drx_rxq();
     q->batch_frames = batch_frames;
     q->max_open = max_open;

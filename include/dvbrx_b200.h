@@ -367,7 +367,7 @@ int drx_fec_decode_device(drx_ldpc* d, drx_bch* b, const int8_t* llr, size_t llr
  * its frames.  A sent batch is decoded on the GPU on its code's stream
  * (copy in, drx_fec_decode_device, copy out); stop 0 stops each frame on
  * its own, stop 1 decodes the batch as one group (the reference's
- * drx_ldpc_decode on the batch).  Batches of different codes overlap on the
+ * drx_ldpc_decode on the batch; batch_frames at most drx_ldpc_lanes()).  Batches of different codes overlap on the
  * GPU.  Frames leave in arrival order (sequence numbers 0, 1, 2, ...).  Like
  * a decoder handle, a queue is used from one host thread at a time. */
 typedef struct drx_rxq drx_rxq;

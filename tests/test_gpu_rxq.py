@@ -161,3 +161,11 @@ def test_rxq_matches_reference_receiver(group):
                 assert it == it_r[k] and ok == ok_r[k], (c, f)
                 assert np.array_equal(cw, words[k]) and bres == res[k], (c, f)
     q.close()
+
+
+def test_rxq_rejects_oversized_groups():
+    with pytest.raises(RuntimeError, match="at most"):
+        D.RxQueue([(D.fec_lookup(1, "1_2"), "1_2")], batch_frames=65, group=True)
+    q = D.RxQueue([(D.fec_lookup(1, "1_2"), "1_2")], batch_frames=1024, group=False)
+    assert q.pop(wait=False) is None and q.pending() == 0
+    q.close()

@@ -636,11 +636,23 @@ def run_b200(args):
                    "frame_iterations_vs_per_frame": float(g_iters.sum()) / max(1, iters_sum),
                    "launch": "one cooperative launch per step, teams of 32 co-resident CTAs per group"}
 
-    # the learned decoder (committed 12-iteration table, int8) with the plain
-    # decoder as fallback, on the same batches and steps
-    learned = None
-    table = None if args.no_learned else load_learned_table()
-    if table is not None:
+    # the learned decoder on the same batches and steps: the committed
+    # 12-iteration table with the plain decoder as fallback (the plain
+    # decoder's FER), and the 30-iteration table in one pass (the plain
+    # decoder's iteration budget, its own FER)
+    def per_point(errors):
+        """frame error rate of each Es/N0 point over the timed steps"""
+        n = [0] * len(llr)
+        e = [0] * len(llr)
+        for k in range(args.steps):
+            b = (args.warmup + k) % len(llr)
+            n[b] += F
+            e[b] += int(errors[k])
+        return [round(e[b] / n[b], 5) if n[b] else None for b in range(len(llr))]
+
+    plain_fer_points = per_point(errs.tolist())
+
+    def run_learned(table, fallback_iters):
         from dvbrx_b200 import train as T
         T.apply_table(dec, table)
         L = int(table["iters"])
@@ -648,7 +660,7 @@ def run_b200(args):
         l_ok = [torch.empty(F, dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
         l_fb = [torch.empty(F, dtype=torch.uint8, device="cuda") for _ in range(args.steps)]
         for k in range(args.warmup):
-            dec.decode_learned(llr[k % len(llr)], L, MAX_ITER, out=outs[0], iters=l_it[0], ok=l_ok[0],
+            dec.decode_learned(llr[k % len(llr)], L, fallback_iters, out=outs[0], iters=l_it[0], ok=l_ok[0],
                                fallback=l_fb[0])
         torch.cuda.synchronize()
         if world > 1:
@@ -656,25 +668,47 @@ def run_b200(args):
         lev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         for k in range(args.steps):
             lev[k][0].record(stream)
-            dec.decode_learned(llr[(args.warmup + k) % len(llr)], L, MAX_ITER, out=outs[k], iters=l_it[k],
+            dec.decode_learned(llr[(args.warmup + k) % len(llr)], L, fallback_iters, out=outs[k], iters=l_it[k],
                                ok=l_ok[k], fallback=l_fb[k])
             lev[k][1].record(stream)
         torch.cuda.synchronize()
         l_ms = max_over_ranks(lev[0][0].elapsed_time(lev[-1][1]), world, "cuda")
-        l_err = sum(int((outs[k] != info[(args.warmup + k) % len(info)]).any(dim=1).sum()) for k in range(args.steps))
+        l_errs = [int((outs[k] != info[(args.warmup + k) % len(info)]).any(dim=1).sum()) for k in range(args.steps)]
         fb_all = torch.stack(l_fb).float()
         lval = aggregate_gbps(world, frames_rank, kldpc, l_ms)
-        learned = {
-            "value": lval, "unit": UNIT, "vs_plain": lval / value, "fer": l_err / frames_rank, "plain_fer": fer,
-            "fallback_frac": float(fb_all.mean()),
-            "avg_iterations_learned_pass": float(torch.stack(l_it).float()[fb_all == 0].mean()) if bool((fb_all == 0).any()) else None,
-            "learned_iters": L, "plain_fallback_max_iter": MAX_ITER, "ms_per_step": l_ms / args.steps,
-            "table": "dvbrx_b200/learned_tables/" + os.path.basename(T.table_path(SHORT, RATE, CONST, L)),
-            "launches_per_step": 3,
-            "decoder": "learned scaled/offset min-sum at int8 (Q8 table per iteration and degree class), "
-                       "frames failing the syndrome re-decoded by the plain decoder on the device",
-        }
         dec.set_learned(None, None, None)
+        res = {
+            "value": lval, "unit": UNIT, "vs_plain": lval / value, "fer": sum(l_errs) / frames_rank, "plain_fer": fer,
+            "fer_per_point": per_point(l_errs), "plain_fer_per_point": plain_fer_points, "esn0_db": ESN0[: len(llr)],
+            "avg_iterations": float(torch.stack(l_it).float().mean()),
+            "plain_avg_iterations": iters_sum / frames_rank,
+            "learned_iters": L, "ms_per_step": l_ms / args.steps,
+            "table": "dvbrx_b200/learned_tables/" + os.path.basename(T.table_path(SHORT, RATE, CONST, L)),
+        }
+        if fallback_iters:
+            res.update({
+                "fallback_frac": float(fb_all.mean()),
+                "avg_iterations_learned_pass": float(torch.stack(l_it).float()[fb_all == 0].mean())
+                if bool((fb_all == 0).any()) else None,
+                "plain_fallback_max_iter": fallback_iters, "launches_per_step": 3,
+                "decoder": "learned scaled/offset min-sum at int8 (Q8 table per iteration and degree class), "
+                           "frames failing the syndrome re-decoded by the plain decoder on the device"})
+        else:
+            res.update({
+                "launches_per_step": 1,
+                "decoder": "learned scaled/offset min-sum at int8 (Q8 table per iteration and degree class), "
+                           "one pass of at most %d iterations with per-frame stopping, no plain decoder" % L})
+        return res
+
+    learned = learned30 = None
+    if not args.no_learned:
+        from dvbrx_b200 import train as T
+        t12 = load_learned_table()
+        if t12 is not None:
+            learned = run_learned(t12, MAX_ITER)
+        t30 = T.load_table(SHORT, RATE, CONST, MAX_ITER)
+        if t30 is not None:
+            learned30 = run_learned(t30, 0)
 
     # the drop-in call as the reference's workers make it: 16 threads, 64-frame calls, host memory
     dropin = None
@@ -744,7 +778,7 @@ def run_b200(args):
             "quality": {"fer": fer, "avg_iterations": iters_sum / frames_rank},
             "roofline": roofline, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "group64": group64,
             "dropin": dropin,
-            "learned": learned,
+            "learned": learned, "learned_30it_one_pass": learned30,
             "mixed_modcod": mix_res, "mixed_modcod_learned": mix_learned, "bch": bch, "demapper": demap,
             "gpu_launches": args.steps,
         }

@@ -139,6 +139,21 @@ __device__ __forceinline__ uint32_t sign_mask(uint32_t w, int k)
     return prmt(w << (k >> 1), 0, (k & 1) ? 0xBB99u : 0xAA88u);
 }
 
+/* The learned magnitudes of the current iteration (learned kernels): byte
+ * 1024 h + 128 k + m = min(learned_mag(m, word of lane h's row and degree
+ * class k), 255) for capped minimums m = 0..127.  A magnitude of 255 or more
+ * saturates every posterior it meets and is capped at 32 in the record, so
+ * the cap at 255 changes no result.  Rebuilt at the start of each learned
+ * iteration (iterate_pair). */
+static __shared__ uint8_t s_learn_lut[2 * kLearnClasses * 128];
+
+/* the learned magnitudes of capped minimums c (both lanes, 0..127) from the
+ * check's class table at index t of s_learn_lut (lane A; lane B at t + 1024) */
+__device__ __forceinline__ uint32_t learned_lut(uint32_t c, uint32_t t)
+{
+    return (uint32_t)s_learn_lut[t + (c & 0xFFFFu)] | (uint32_t)s_learn_lut[t + 1024u + (c >> 16)] << 16;
+}
+
 /* WIDE: the kernel's records are 16 bytes (its degree bound is above 16).
  * PO: the parity posteriors (slots 0 and 1) are not in shared memory; the
  * layer loop hands their two-byte words in and takes the new ones back. */
@@ -304,8 +319,8 @@ struct PairCheckKey {
         }
     }
 
-    /* the cap at 127 and offset 1, or the learned scale and offset of each
-     * lane's iteration (lpA, lpB); the outgoing candidates +-mn0, +-mn1 with
+    /* the cap at 127 and offset 1, or the learned magnitudes of each lane's
+     * iteration (lpA: the check's class table, learned_lut); the outgoing candidates +-mn0, +-mn1 with
      * the check's sign parity applied (a0, a1 for a slot whose value is
      * positive, b0 = -a0, b1 = -a1 otherwise) and the record's magnitudes.
      * Only threads with `take` keep the result: the level steps run it on
@@ -316,8 +331,8 @@ struct PairCheckKey {
         const uint32_t c1 = __vmins2((min1 >> 5) & 0x07FF07FFu, 0x007F007Fu);
         uint32_t m0, m1;
         if (learned) {
-            m0 = (uint32_t)learned_mag(c0 & 0xFFFF, lpA) | (uint32_t)learned_mag(c0 >> 16, lpB) << 16;
-            m1 = (uint32_t)learned_mag(c1 & 0xFFFF, lpA) | (uint32_t)learned_mag(c1 >> 16, lpB) << 16;
+            m0 = learned_lut(c0, lpA);
+            m1 = learned_lut(c1, lpA);
         } else {
             m0 = __viaddmax_s16x2(c0, 0xFFFFFFFFu, 0u);
             m1 = __viaddmax_s16x2(c1, 0xFFFFFFFFu, 0u);
@@ -548,17 +563,16 @@ struct PairCheckMin {
         }
     }
 
-    /* the cap at 127 and offset 1, or the learned scale and offset of each
-     * lane's iteration (lpA, lpB).  Only threads with `take` keep the result:
-     * the level steps run it on whole warps */
+    /* the cap at 127 and offset 1, or the learned magnitudes of each lane's
+     * iteration (lpA: the check's class table, learned_lut).  Only threads
+     * with `take` keep the result: the level steps run it on whole warps */
     __device__ __forceinline__ void finish(bool take, bool learned, uint32_t lpA, uint32_t lpB)
     {
         const uint32_t c1 = min1, c0 = min0;
         uint32_t m0, m1;
         if (learned) {
-            const uint32_t k0 = __vmins2(c0, 0x007F007Fu), k1 = __vmins2(c1, 0x007F007Fu);
-            m0 = (uint32_t)learned_mag(k0 & 0xFFFF, lpA) | (uint32_t)learned_mag(k0 >> 16, lpB) << 16;
-            m1 = (uint32_t)learned_mag(k1 & 0xFFFF, lpA) | (uint32_t)learned_mag(k1 >> 16, lpB) << 16;
+            m0 = learned_lut(__vmins2(c0, 0x007F007Fu), lpA);
+            m1 = learned_lut(__vmins2(c1, 0x007F007Fu), lpA);
         } else {
             m0 = __viaddmax_s16x2(__vmins2(c0, 0x007F007Fu), 0xFFFFFFFFu, 0u);
             m1 = __viaddmax_s16x2(__vmins2(c1, 0x007F007Fu), 0xFFFFFFFFu, 0u);
@@ -851,14 +865,11 @@ __device__ __forceinline__ void layer_pair(const PairFrame& fr, const DevCode& c
     const int t = threadIdx.x;
     const bool active = t < kQCp;
     const int j = t;
-    /* learned scale / offset words of the check for both lanes */
+    /* the check's learned class table (an index into s_learn_lut) */
     auto lwords = [&](uint32_t& a, uint32_t& b) {
         a = b = 0;
-        if (LEARNED) {
-            const int k = s_learn_cls[(EXACT ? DM : cnt + 2) - ((i | j) == 0)];
-            a = s_learn_tab[lA + k];
-            b = s_learn_tab[lB + k];
-        }
+        if (LEARNED)
+            a = 128u * (uint32_t)s_learn_cls[(EXACT ? DM : cnt + 2) - ((i | j) == 0)];
     };
     using Ck = PairCheck<DM, EXACT, LS, WIDE, PO, KEYS>;
     Ck ck;
@@ -933,6 +944,14 @@ __device__ void iterate_pair(const DevCode& c, const PairFrame& fr, void* msgv, 
      * i + 1 (loaded two layers ahead), and of (i - 1, j), which the previous
      * layer of this thread wrote */
     uint32_t pnext = 0, pnext2 = 0, carry = 0;
+    if (LEARNED) {
+        /* this iteration's learned magnitudes: lane A's row lA, lane B's lB */
+        for (int e = t; e < 2 * kLearnClasses * 128; e += blockDim.x) {
+            const int h = e / (kLearnClasses * 128), k = (e / 128) % kLearnClasses;
+            s_learn_lut[e] = (uint8_t)min(learned_mag(e % 128, s_learn_tab[(h ? lB : lA) + k]), 255);
+        }
+        __syncthreads();
+    }
     if (active) {
         rn = __ldcg(msg + j);
         mn = __ldg(c.lmeta + j);

@@ -218,14 +218,17 @@ def validate(model, vset):
 
 def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, lr, seed, log=None,
           weights="uniform", val_points=None, int8_inputs=False, decodable_iters=0, select_points=None,
-          select_frames=1024, eval_every=20):
+          select_frames=1024, eval_every=20, floor_points=None, floor_frames=4096, max_scale=4.0):
     """Adam on the fp32 masters of the FP16 tables, initialised to the
     plain decoder (scale 1, offset 1).  int8_inputs / decodable_iters: the
     minibatches of int8_minibatch.  select_points: Es/N0 points of a fixed
     selection set; every eval_every steps the int8 learned decoder's FER at
     `iters` iterations is measured there, and the model keeps the best tables
     seen (the plain decoder's to start with), so that the result is never
-    worse than the plain decoder on that set.  Returns (model, history)."""
+    worse than the plain decoder on that set.  floor_points: Es/N0 points above
+    the waterfall (floor_frames frames each) where a table is kept only if it
+    fails no more frames than the plain decoder does.  max_scale: the upper
+    bound of every scale.  Returns (model, history)."""
     world, rank = dist_world()
     torch.manual_seed(seed)
     rng = np.random.default_rng(rank_seed(seed, rank))
@@ -237,6 +240,8 @@ def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, l
     opt = torch.optim.Adam(model.parameters(), lr=lr)
     hist = []
     sset = int8_selection_set(model.dec, select_points, select_frames, constellation) if select_points else None
+    fset = int8_selection_set(model.dec, floor_points, floor_frames, constellation, seed=8765) if floor_points else None
+    floor0 = int8_fer(model.dec, model.beta, model.alpha, model.cod, fset, iters)[0] if fset else 0.0
     best = None
     if sset:
         f0, i0 = int8_fer(model.dec, model.beta, model.alpha, model.cod, sset, iters)
@@ -259,14 +264,19 @@ def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, l
         average_gradients(list(model.parameters()), world)
         opt.step()
         with torch.no_grad():
-            model.beta.clamp_(0.0, 4.0)
+            model.beta.clamp_(0.0, max_scale)
         ev1.record()
         torch.cuda.synchronize()
         rec = {"step": k, "loss": float(loss.detach()), "ms": ev0.elapsed_time(ev1)}
         if sset and ((k + 1) % eval_every == 0 or k == steps - 1):
             f, i = int8_fer(model.dec, model.beta, model.alpha, model.cod, sset, iters)
             rec.update({"select_fer": f, "select_avg_iters": i})
-            if (f, i) < (best[0], best[1]):
+            ok = True
+            if fset:
+                ff = int8_fer(model.dec, model.beta, model.alpha, model.cod, fset, iters)[0]
+                rec["floor_fer"] = ff
+                ok = ff <= floor0
+            if ok and (f, i) < (best[0], best[1]):
                 best = (f, i, model.beta.detach().clone(), model.alpha.detach().clone(), k)
         hist.append(rec)
         if log and (k % 10 == 0 or k == steps - 1):
@@ -277,6 +287,9 @@ def train(short_frame, rate, constellation, iters, batch, es_lo, es_hi, steps, l
             model.alpha.copy_(best[3])
         model.selection.update({"fer": best[0], "avg_iters": best[1], "step": best[4],
                                 "points": list(select_points), "frames_per_point": select_frames})
+        if fset:
+            model.selection.update({"floor_points": list(floor_points), "floor_frames_per_point": floor_frames,
+                                    "plain_floor_fer": floor0})
         if log:
             log(json.dumps({"selection_best": model.selection}))
     model.validation = validate(model, vset)
@@ -296,7 +309,8 @@ def export(model, meta):
 def evaluate(short_frame, rate, constellation, table, es_list, nframes, learned_iters, plain_iters, seed=7):
     """FER of plain@plain_iters, plain@learned_iters, learned@learned_iters
     and learned + plain fallback on the same frames, with device-timed
-    Gbit/s of the plain and the learned + fallback decodes."""
+    Gbit/s of the plain, the learned + fallback and the learned-only
+    (one pass, no fallback) decodes."""
     p = _params(short_frame, rate)
     dec = Ldpc(p, rate)
     apply_table(dec, table)
@@ -304,7 +318,7 @@ def evaluate(short_frame, rate, constellation, table, es_list, nframes, learned_
     for k, es in enumerate(es_list):
         llr, info, _ = dec.generate(nframes, float(es), seed=seed + 1000 * k, constellation=constellation, info=True)
         res = {"esn0_db": float(es)}
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         dec.decode_device(llr, plain_iters)  # warm-up
         dec.decode_learned(llr, learned_iters, plain_iters)
         torch.cuda.synchronize()
@@ -316,6 +330,9 @@ def evaluate(short_frame, rate, constellation, table, es_list, nframes, learned_
         torch.cuda.synchronize()
         sb, si, so = dec.decode_device(llr, learned_iters)
         ob, oi, oo, _ = dec.decode_learned(llr, learned_iters, 0)
+        ev[3].record()
+        dec.decode_learned(llr, learned_iters, 0, out=ob, iters=oi, ok=oo)
+        ev[4].record()
         torch.cuda.synchronize()
 
         def fer(bits):
@@ -328,12 +345,14 @@ def evaluate(short_frame, rate, constellation, table, es_list, nframes, learned_
 
         t_plain = ev[0].elapsed_time(ev[1]) * 1e-3
         t_learn = ev[1].elapsed_time(ev[2]) * 1e-3
+        t_only = ev[3].elapsed_time(ev[4]) * 1e-3
         res.update({
             "plain_fer": fer(pb), "plain_ber": ber(pb), "plain_avg_iters": float(pi.float().mean()),
             "plain_short_fer": fer(sb),
             "learned_only_fer": fer(ob), "learned_only_avg_iters": float(oi.float().mean()),
             "learned_fer": fer(lb), "learned_ber": ber(lb), "fallback_frac": float(fb.float().mean()),
             "plain_gbps": nframes * p.kldpc / t_plain / 1e9, "learned_gbps": nframes * p.kldpc / t_learn / 1e9,
+            "learned_only_gbps": nframes * p.kldpc / t_only / 1e9,
         })
         rows.append(res)
     return rows
@@ -364,6 +383,10 @@ def main(argv=None):
     ap.add_argument("--select", type=float, nargs="*", default=None,
                     help="Es/N0 points of the model-selection set (int8 FER at --iters iterations)")
     ap.add_argument("--select-frames", type=int, default=1024)
+    ap.add_argument("--select-floor", type=float, nargs="*", default=None,
+                    help="Es/N0 points above the waterfall where a kept table fails no more frames than plain")
+    ap.add_argument("--floor-frames", type=int, default=4096)
+    ap.add_argument("--max-scale", type=float, default=4.0, help="upper bound of the trained scales")
     ap.add_argument("--select-offsets", type=float, nargs="*", default=None,
                     help="--all-s2: selection points as offsets (dB) from each rate's QEF Es/N0")
     ap.add_argument("--all-s2", action="store_true",
@@ -426,7 +449,8 @@ def main(argv=None):
     t0 = time.time()
     model, hist = train(a.short, a.rate, a.const, a.iters, a.batch, a.es[0], a.es[1], a.steps, a.lr, a.seed, log,
                         a.weights, a.val, int8_inputs=a.int8_inputs, decodable_iters=a.decodable,
-                        select_points=a.select, select_frames=a.select_frames)
+                        select_points=a.select, select_frames=a.select_frames, floor_points=a.select_floor,
+                        floor_frames=a.floor_frames, max_scale=a.max_scale)
     wall = time.time() - t0
     ms = [h["ms"] for h in hist[1:]] or [hist[0]["ms"]]
     meta = {"short": a.short, "rate": a.rate, "constellation": a.const, "es": a.es, "batch": a.batch,

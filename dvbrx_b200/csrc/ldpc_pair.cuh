@@ -320,9 +320,10 @@ struct PairCheckKey {
     }
 
     /* the cap at 127 and offset 1, or the learned magnitudes of each lane's
-     * iteration (lpA: the check's class table, learned_lut); the outgoing candidates +-mn0, +-mn1 with
-     * the check's sign parity applied (a0, a1 for a slot whose value is
-     * positive, b0 = -a0, b1 = -a1 otherwise) and the record's magnitudes.
+     * iteration (lpA: the check's class table, learned_lut; lpB unused); the
+     * outgoing candidates +-mn0, +-mn1 with the check's sign parity applied
+     * (a0, a1 for a slot whose value is positive, b0 = -a0, b1 = -a1
+     * otherwise) and the record's magnitudes.
      * Only threads with `take` keep the result: the level steps run it on
      * whole warps */
     __device__ __forceinline__ void finish(bool take, bool learned, uint32_t lpA, uint32_t lpB)
@@ -564,8 +565,9 @@ struct PairCheckMin {
     }
 
     /* the cap at 127 and offset 1, or the learned magnitudes of each lane's
-     * iteration (lpA: the check's class table, learned_lut).  Only threads
-     * with `take` keep the result: the level steps run it on whole warps */
+     * iteration (lpA: the check's class table, learned_lut; lpB unused).
+     * Only threads with `take` keep the result: the level steps run it on
+     * whole warps */
     __device__ __forceinline__ void finish(bool take, bool learned, uint32_t lpA, uint32_t lpB)
     {
         const uint32_t c1 = min1, c0 = min0;

@@ -72,6 +72,32 @@ def test_random_tables_match_cpu_model(short, rate, es, iters):
         assert np.array_equal(ok.cpu().numpy(), want[2]), (rate, v)
 
 
+@pytest.mark.parametrize("short,rate,es,iters", [(1, "1_2", 1.6, 6), (0, "3_5", 2.7, 5)])
+def test_large_scales_match_cpu_model(short, rate, es, iters):
+    """Scales up to 3.9 make learned magnitudes above 255, where the pair
+    kernel's per-iteration table caps them (a magnitude of 255 or more
+    saturates every posterior and is capped at 32 in the record): bits,
+    iterations and flags still equal the CPU model, which does not cap."""
+    dec = D.Ldpc(D.fec_lookup(short, rate), rate)
+    n = 24 if short else 8
+    llr_np = awgn_frames(short, rate, n, es, seed=23)
+    llr = torch.from_numpy(llr_np).cuda()
+    nclass, cod = classes(short, rate)
+    rng = np.random.default_rng(iters + 100)
+    scale = rng.uniform(1.5, 3.9, size=(iters, nclass)).astype(np.float32)
+    offset = rng.uniform(-2.0, 3.0, size=(iters, nclass)).astype(np.float32)
+    assert float(scale.max()) * 127 - float(offset.min()) > 255  # the cap is reached
+    dec.set_learned(scale, offset, cod)
+    want = oracle.OrcCode(short, rate).decode_frames_learned(llr_np, iters, scale, offset, cod)
+    for v in variants(dec):
+        dec.set_variant(v)
+        bits, it, ok, fb = dec.decode_learned(llr, iters, 0)
+        assert np.array_equal(bits.cpu().numpy(), want[0]), (rate, v)
+        assert np.array_equal(it.cpu().numpy(), want[1]), (rate, v)
+        assert np.array_equal(ok.cpu().numpy(), want[2]), (rate, v)
+    dec.close()
+
+
 @pytest.mark.parametrize("short,rate,es,iters,n", [(1, "1_2", 1.4, 8, 64), (0, "3_5", 2.6, 11, 32)])
 def test_fallback_redecodes_failing_frames(short, rate, es, iters, n):
     dec = D.Ldpc(D.fec_lookup(short, rate), rate)

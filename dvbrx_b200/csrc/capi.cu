@@ -640,10 +640,9 @@ drx_ldpc* drx_ldpc_new(const drx_fec_params* p, const char* rate)
         d->pair_smem = smem_of(d->pair_kid);
         d->pair_ctas_per_sm = decode_pair_ctas_per_sm(d->pair_kid, d->pair_smem);
         /* a two-CTA twin when it makes more CTAs resident: all posteriors in
-         * shared memory if they leave room, else the parity-out one (unless
-         * the code measured faster on the one-CTA kernel) */
+         * shared memory if they leave room, else the parity-out one */
         const int base = d->pair_kid;
-        for (int pm = 1; pm <= 2 && !pair_one_cta_preferred(d->code); pm++) {
+        for (int pm = 1; pm <= 2; pm++) {
             const int tw = pair_kernel_twin(base, pm);
             if (tw < 0)
                 continue;

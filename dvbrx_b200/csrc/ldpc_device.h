@@ -156,8 +156,6 @@ int pair_kernel_id(const Code& c);
  * posterior in shared memory, pm 2 keeps the parity posteriors in the CTA's
  * global slab and in registers (about half the shared memory); -1 if none */
 int pair_kernel_twin(int kid, int pm);
-/* the code runs faster on the one-CTA kernel than on its twin (measured) */
-bool pair_one_cta_preferred(const Code& c);
 size_t decode_pair_smem_bytes(int N, int K, int nent, int nsteps, int q, int kid);
 size_t decode_pair_msg_bytes(int R, int kid);
 int decode_pair_ctas_per_sm(int kid, size_t smem);

@@ -94,17 +94,6 @@ bool pair_kernel_shape(int kid, int* a, int* b, int* gdm, int* ls, int* pm)
     return true;
 }
 
-/* Codes whose one-CTA kernel measured faster than its two-CTA twin, which
- * the occupancy rule would pick (ns per non-converging frame-iteration on a
- * B200, 2048 QPSK frames at -4 dB): normal 1/2 (EN 302 307-1 Table B.4), 349
- * against 376.  Its checks have degree 7, so the parity-out twin moves two of
- * the seven links of every check through the CTA's global slab.  Every other
- * code measured its twin faster, or has none. */
-bool pair_one_cta_preferred(const Code& c)
-{
-    return c.table_name == "DVB_S2_TABLE_B4";
-}
-
 /* the twin of a mode-0 kernel in mode pm (1 or 2), -1 if it has none */
 int pair_kernel_twin(int kid, int pm)
 {
